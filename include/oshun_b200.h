@@ -1,0 +1,152 @@
+/* oshun_b200 — C ABI of the B200 (sm_100a) implementation of OSHUN's
+ * per-time-step hot path: the RK4 Vlasov-Maxwell stage on the spherical-
+ * harmonic distribution f_lm(p,x,y) and the Fokker-Planck collision step.
+ *
+ * Plain C linkage, plain pointers and sizes.  Every entry point returns an
+ * oshun_status code; none throws or exits.  Each entry point names the
+ * reference interface it replaces (paths are within the OSHUN repository).
+ *
+ * Host data layout (the reference's storage order without guard cells):
+ *   harmonics: complex128, [Nh][numy][numx][nump], harmonic index ind(l,m)
+ *              (OSHUN-1/def-State.cpp:420-427), Nh = (m0+1)(2 l0-m0+2)/2
+ *              (OSHUN-1/def-State.cpp:417), p fastest
+ *              (OSHUN-1/matrices.h:714-716)
+ *   fields:    complex128, [6][numy][numx] in the order Ex Ey Ez Bx By Bz
+ *              (OSHUN-1/decl-state.h:120-125)
+ * Boundaries are periodic in x and y; the reference's RKLevel = 4 guard
+ * cells are not stored (a periodic stencil gives the same interior values,
+ * OSHUN-1/def-Input.cpp:156-164).
+ */
+#ifndef OSHUN_B200_H
+#define OSHUN_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OSHUN_ABI_VERSION 1
+
+typedef enum oshun_status {
+    OSHUN_OK = 0,
+    OSHUN_ERR_ARG = 1,          /* bad pointer, size or configuration value */
+    OSHUN_ERR_UNSUPPORTED = 2,  /* configuration outside the compiled range */
+    OSHUN_ERR_CUDA = 3,         /* a CUDA runtime call failed (see oshun_last_error) */
+    OSHUN_ERR_NONREAL = 4,      /* upload: an m=0 harmonic or a field has an imaginary part */
+    OSHUN_ERR_NUMERIC = 5,      /* a step produced NaN/Inf (see oshun_status_flags) */
+    OSHUN_ERR_NO_DEVICE = 6     /* no CUDA device, or not an sm_100 device */
+} oshun_status;
+
+typedef enum oshun_precision {
+    OSHUN_FP64 = 0,       /* every operator in IEEE FP64: the drop-in */
+    OSHUN_FP32_SPLIT = 1  /* f_lm (l >= 1), fields and their arithmetic in FP32; f00, the
+                             Rosenbluth integrals, the collision solves and the current
+                             reduction in FP64 */
+} oshun_precision;
+
+/* flags */
+#define OSHUN_FLAG_FIX_YADV_CHAIN 0x1  /* drop the reference's y-advection coefficient
+                                          factor for m >= 2 (see DESIGN of the RHS) */
+
+/* Run configuration: the input-deck fields the hot path reads
+ * (OSHUN-1/decl-input.h:59-138, derived values as in
+ * OSHUN-1/def-Input.cpp:79,156-164,313-334). */
+typedef struct oshun_cfg {
+    int l0, m0;              /* harmonic truncation, 0 <= m0 <= l0 */
+    int nump, numx, numy;    /* interior cells; numy = 1 for a 1D run */
+    double pmin, pmax;       /* p_i = i (pmax-pmin)/(nump-1) + pmin (matrices.h:860-866) */
+    double xmin, xmax;       /* dx = (xmax-xmin)/(numx-1) (the reference's xglob axis) */
+    double ymin, ymax;       /* dy likewise; unused when numy = 1 */
+    double dt;               /* RK4 step h (Runge_Kutta_4 ctor, def-RK.cpp:60-61) */
+    double t0;               /* start time of the RK, e-e and implicit clocks */
+    double small_dt;         /* bound on the f00 e-e substep (def-FokkerPlanck.cpp:598) */
+    int NB_algorithms;       /* low-v cells of the e-e flux (def-FokkerPlanck.cpp:241) */
+    int if_tridiagonal;      /* 1: Thomas solve; 0: dense matrix + Gauss-Seidel */
+    int if_implicit1D;       /* 1: implicit collisions on m = 0 only (f1_loop1D/flm_loop1D) */
+    double density_np;       /* electron density in 1/cm^3 (Coulomb logarithms) */
+    double Zeta;             /* ion charge */
+    int precision;           /* oshun_precision */
+    int flags;               /* OSHUN_FLAG_* */
+} oshun_cfg;
+
+typedef struct oshun_ctx* oshun_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Allocates the device state for cfg and builds the operator tables.
+ * Replaces the construction of Stat, Runge_Kutta_4, Explicit_EC_FP and
+ * Euler_Backward (OSHUN-1/main.cpp:147-199; def-State.cpp:533-538;
+ * def-RK.cpp:49-62; def-FokkerPlanck.cpp:568-585, 1258-1266). */
+int oshun_create(const oshun_cfg* cfg, oshun_handle* out);
+int oshun_destroy(oshun_handle h);
+
+/* Runs the handle's work on this cudaStream_t (passed as void*; NULL = the
+ * handle's own stream). */
+int oshun_set_stream(oshun_handle h, void* stream);
+int oshun_synchronize(oshun_handle h);
+
+/* ---- state transfer ------------------------------------------------------ */
+
+/* Host -> device copy of the state.  Replaces filling a Stat
+ * (Setup_Y::initialize, OSHUN-1/def-Setup.cpp:293-471, or
+ * Restart_Facility::Read, def-Export.cpp:733-766).  m = 0 harmonics and the
+ * fields must be real (OSHUN_ERR_NONREAL otherwise): every reference operator
+ * maps real m = 0 harmonics and real fields to real values. */
+int oshun_upload(oshun_handle h, const double* harmonics, const double* fields);
+/* Device -> host copy of the state (replaces reading Stat, e.g.
+ * Restart_Facility::Write, def-Export.cpp:768-836). */
+int oshun_download(oshun_handle h, double* harmonics, double* fields);
+
+/* ---- operators ------------------------------------------------------------ */
+
+/* slope = Actions::Adv(state) (OSHUN-1/def-Actions.cpp:73-94): E-field,
+ * current, Ampere, advection, B-field, Faraday, CLEAN_LOW_PC.  Writes the
+ * slope to host buffers in the state layout; the state is unchanged. */
+int oshun_rhs(oshun_handle h, double* slope_harmonics, double* slope_fields);
+
+/* One RK4 step of h = cfg.dt: Runge_Kutta_4::advance_p1
+ * (OSHUN-1/def-RK.cpp:110-145).  Advances the RK clock. */
+int oshun_rk4_step(oshun_handle h);
+
+/* Explicit_EC_FP::loop(t_new) (OSHUN-1/def-FokkerPlanck.cpp:590-625): f00
+ * e-e collisions, floor((t_new - t_ee)/small_dt)+1 RK4 substeps per cell. */
+int oshun_collide_ee(oshun_handle h, double t_new);
+
+/* Euler_Backward::advance_1(t_new) (OSHUN-1/def-FokkerPlanck.cpp:1270-1286):
+ * implicit step of f10 (and f11 in 2D) over t_new - t_eb. */
+int oshun_collide_f1(oshun_handle h, double t_new);
+/* Euler_Backward::advance_lm(t_new) (OSHUN-1/def-FokkerPlanck.cpp:1290-1304):
+ * implicit step of every f_lm with l >= 2; sets t_eb = t_new. */
+int oshun_collide_flm(oshun_handle h, double t_new);
+
+/* nsteps of the reference's small-step sequence (OSHUN-1/main.cpp:77-107):
+ * rk4.advance_p1; ee.loop(t); eb.advance_1(t); eb.advance_lm(t).  Runs as a
+ * CUDA graph once captured.  `collisions` = 0 skips the collision calls. */
+int oshun_step(oshun_handle h, int nsteps, int collisions);
+
+/* ---- queries -------------------------------------------------------------- */
+
+/* RK clock (Runge_Kutta_4::time, OSHUN-1/def-RK.cpp:76). */
+int oshun_time(oshun_handle h, double* t);
+/* Status word: bit 0 = a Gauss-Seidel solve found its matrix not diagonally
+ * dominant and kept f (the reference's WARNING, def-FokkerPlanck.cpp:1027-1030);
+ * bit 1 = NaN/Inf in the state.  *count = skipped solves since the last call.
+ * Reading clears the word. */
+int oshun_status_flags(oshun_handle h, int* flags, long long* count);
+/* Device pointers of the state planes for zero-copy use: the f00 plane
+ * (FP64, [numy][numx][nump]), the other planes (see oshun_plane_layout), the
+ * 6 field planes; sizes in bytes. */
+int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields,
+                       size_t* planes_bytes, size_t* fields_bytes);
+/* Plane index of the real part of harmonic (l,m) in `planes` (the imaginary
+ * part, m > 0, follows it), or -1 for (0,0), which lives in `f00`. */
+int oshun_plane_index(oshun_handle h, int l, int m, int* plane);
+/* Human-readable message of the last error on this thread. */
+const char* oshun_last_error(void);
+int oshun_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

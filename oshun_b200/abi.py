@@ -1,0 +1,202 @@
+"""ctypes binding of liboshun_b200.so (the C ABI in include/oshun_b200.h).
+
+Used by the tests and bench.py to drive the CUDA path exactly as a foreign
+caller would.  There is no fallback: if the library is missing or no B200 is
+present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboshun_b200.so")
+
+OSHUN_FP64 = 0
+OSHUN_FP32_SPLIT = 1
+OSHUN_FLAG_FIX_YADV_CHAIN = 0x1
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4: "ERR_NONREAL",
+          5: "ERR_NUMERIC", 6: "ERR_NO_DEVICE"}
+
+EXPORTED = [
+    "oshun_create", "oshun_destroy", "oshun_set_stream", "oshun_synchronize", "oshun_upload",
+    "oshun_download", "oshun_rhs", "oshun_rk4_step", "oshun_collide_ee", "oshun_collide_f1",
+    "oshun_collide_flm", "oshun_step", "oshun_time", "oshun_status_flags", "oshun_device_state",
+    "oshun_plane_index", "oshun_last_error", "oshun_abi_version",
+]
+
+
+class OshunCfg(ctypes.Structure):
+    _fields_ = [
+        ("l0", ctypes.c_int), ("m0", ctypes.c_int),
+        ("nump", ctypes.c_int), ("numx", ctypes.c_int), ("numy", ctypes.c_int),
+        ("pmin", ctypes.c_double), ("pmax", ctypes.c_double),
+        ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+        ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
+        ("dt", ctypes.c_double), ("t0", ctypes.c_double), ("small_dt", ctypes.c_double),
+        ("NB_algorithms", ctypes.c_int), ("if_tridiagonal", ctypes.c_int), ("if_implicit1D", ctypes.c_int),
+        ("density_np", ctypes.c_double), ("Zeta", ctypes.c_double),
+        ("precision", ctypes.c_int), ("flags", ctypes.c_int),
+    ]
+
+
+class OshunError(RuntimeError):
+    def __init__(self, code: int, what: str, msg: str):
+        super().__init__(f"{what}: {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the library once; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is not built (python -m oshun_b200.build)")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.oshun_create.argtypes = [ctypes.POINTER(OshunCfg), ctypes.POINTER(vp)]
+    lib.oshun_destroy.argtypes = [vp]
+    lib.oshun_set_stream.argtypes = [vp, vp]
+    lib.oshun_synchronize.argtypes = [vp]
+    lib.oshun_upload.argtypes = [vp, vp, vp]
+    lib.oshun_download.argtypes = [vp, vp, vp]
+    lib.oshun_rhs.argtypes = [vp, vp, vp]
+    lib.oshun_rk4_step.argtypes = [vp]
+    lib.oshun_collide_ee.argtypes = [vp, ctypes.c_double]
+    lib.oshun_collide_f1.argtypes = [vp, ctypes.c_double]
+    lib.oshun_collide_flm.argtypes = [vp, ctypes.c_double]
+    lib.oshun_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.oshun_time.argtypes = [vp, dp]
+    lib.oshun_status_flags.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)]
+    lib.oshun_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                       ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+    lib.oshun_plane_index.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.oshun_last_error.restype = ctypes.c_char_p
+    lib.oshun_abi_version.restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def make_cfg(**kw) -> OshunCfg:
+    c = OshunCfg()
+    defaults = dict(t0=0.0, precision=OSHUN_FP64, flags=0, NB_algorithms=4, if_tridiagonal=1,
+                    if_implicit1D=1, density_np=1e21, Zeta=1.0, ymin=0.0, ymax=1.0, small_dt=1.0)
+    defaults.update(kw)
+    for name, _ in OshunCfg._fields_:
+        if name not in defaults:
+            raise KeyError(f"oshun_cfg field {name} missing")
+        setattr(c, name, defaults[name])
+    return c
+
+
+class Handle:
+    """One oshun_handle: the device state of one run and its operators."""
+
+    def __init__(self, **cfg):
+        self.lib = load()
+        self.cfg = make_cfg(**cfg)
+        self._h = ctypes.c_void_p()
+        self._check(self.lib.oshun_create(ctypes.byref(self.cfg), ctypes.byref(self._h)), "oshun_create")
+        c = self.cfg
+        self.nh = ((c.m0 + 1) * (2 * c.l0 - c.m0 + 2)) // 2
+        self.fshape = (self.nh, c.numy, c.numx, c.nump)
+        self.fldshape = (6, c.numy, c.numx)
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            raise OshunError(rc, what, self.lib.oshun_last_error().decode())
+
+    def close(self) -> None:
+        if self._h:
+            self.lib.oshun_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+        return ctypes.c_void_p(a.ctypes.data)
+
+    def upload(self, f: np.ndarray, fields: np.ndarray) -> None:
+        f = np.ascontiguousarray(f, np.complex128)
+        fields = np.ascontiguousarray(fields, np.complex128)
+        assert f.shape == self.fshape and fields.shape == self.fldshape
+        self._check(self.lib.oshun_upload(self._h, self._ptr(f), self._ptr(fields)), "oshun_upload")
+
+    def upload_ptr(self, f_ptr: int, fields_ptr: int) -> None:
+        self._check(self.lib.oshun_upload(self._h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(fields_ptr)),
+                    "oshun_upload")
+
+    def download(self):
+        f = np.empty(self.fshape, np.complex128)
+        fields = np.empty(self.fldshape, np.complex128)
+        self._check(self.lib.oshun_download(self._h, self._ptr(f), self._ptr(fields)), "oshun_download")
+        return f, fields
+
+    def download_ptr(self, f_ptr: int, fields_ptr: int) -> None:
+        self._check(self.lib.oshun_download(self._h, ctypes.c_void_p(f_ptr), ctypes.c_void_p(fields_ptr)),
+                    "oshun_download")
+
+    def rhs(self):
+        f = np.empty(self.fshape, np.complex128)
+        fields = np.empty(self.fldshape, np.complex128)
+        self._check(self.lib.oshun_rhs(self._h, self._ptr(f), self._ptr(fields)), "oshun_rhs")
+        return f, fields
+
+    def rk4_step(self) -> None:
+        self._check(self.lib.oshun_rk4_step(self._h), "oshun_rk4_step")
+
+    def collide_ee(self, t_new: float) -> None:
+        self._check(self.lib.oshun_collide_ee(self._h, t_new), "oshun_collide_ee")
+
+    def collide_f1(self, t_new: float) -> None:
+        self._check(self.lib.oshun_collide_f1(self._h, t_new), "oshun_collide_f1")
+
+    def collide_flm(self, t_new: float) -> None:
+        self._check(self.lib.oshun_collide_flm(self._h, t_new), "oshun_collide_flm")
+
+    def step(self, nsteps: int, collisions: bool = True) -> None:
+        self._check(self.lib.oshun_step(self._h, nsteps, 1 if collisions else 0), "oshun_step")
+
+    def synchronize(self) -> None:
+        self._check(self.lib.oshun_synchronize(self._h), "oshun_synchronize")
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._check(self.lib.oshun_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "oshun_set_stream")
+
+    @property
+    def time(self) -> float:
+        t = ctypes.c_double()
+        self._check(self.lib.oshun_time(self._h, ctypes.byref(t)), "oshun_time")
+        return t.value
+
+    def status_flags(self):
+        fl = ctypes.c_int()
+        cnt = ctypes.c_longlong()
+        self._check(self.lib.oshun_status_flags(self._h, ctypes.byref(fl), ctypes.byref(cnt)), "oshun_status_flags")
+        return fl.value, cnt.value
+
+    def device_state(self):
+        f00, pl, fl = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        pb, fb = ctypes.c_size_t(), ctypes.c_size_t()
+        self._check(self.lib.oshun_device_state(self._h, ctypes.byref(f00), ctypes.byref(pl), ctypes.byref(fl),
+                                                ctypes.byref(pb), ctypes.byref(fb)), "oshun_device_state")
+        return f00.value, pl.value, fl.value, pb.value, fb.value

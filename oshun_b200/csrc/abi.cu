@@ -1,0 +1,800 @@
+// C ABI of liboshun_b200 (include/oshun_b200.h): handle lifetime, operator
+// tables, state transfer, the RK4 step driver, the collision driver and the
+// captured-graph step loop.
+//
+// Device state (per handle):
+//   f00 plane      FP64 [numy][numx][nump]
+//   planes         every l >= 1 harmonic as 1 (m = 0) or 2 (m > 0, Re then Im)
+//                  real planes [numy][numx][nump], harmonics in ind(l,m) order;
+//                  FP64, or FP32 in OSHUN_FP32_SPLIT
+//   fields         6 real planes [numy][numx] (Ex Ey Ez Bx By Bz)
+// m = 0 harmonics and the fields are stored real: every reference operator
+// keeps them real (the couplings into m = 0 take real parts,
+// OSHUN-1/def-VlasovMax.cpp:386,394,614,878), so their imaginary parts are
+// identically zero.
+//
+// Four copies of the state rotate through an RK4 step (Runge_Kutta_4 keeps
+// Y, Y0, Y1, Yh; def-RK.cpp:56): set `cur` is Y0 (stage-1 input), set `nxt`
+// is the accumulator Y that becomes the new state, sets 2 and 3 carry the
+// stage inputs.  `cur` and `nxt` swap after each step.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "oshun_internal.h"
+
+namespace oshun {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
+struct Clock {
+    double t, t_ee, t_eb;
+};
+
+// ---- small kernels ---------------------------------------------------------
+
+// case layout (complex128 per harmonic) -> planes; flags nonzero imaginary
+// parts of m = 0 harmonics and fields
+template <typename TS>
+__global__ void scatter_kernel(const double2* __restrict__ src, double* f00, TS* planes, TS* fields,
+                               const int* __restrict__ hplane, long long pstride, int nh, long long cells,
+                               int* flag) {
+    const long long total = (long long)nh * pstride + 6 * cells;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double2 v = src[i];
+        if (i < (long long)nh * pstride) {
+            const int h = (int)(i / pstride);
+            const long long off = i - (long long)h * pstride;
+            const int q = hplane[h];
+            if (q < 0) {                               // f00
+                f00[off] = v.x;
+                if (v.y != 0.0) *flag = 1;
+            } else if (q >= 0 && hplane[nh + h]) {     // m > 0: Re, Im
+                planes[(long long)q * pstride + off] = (TS)v.x;
+                planes[(long long)(q + 1) * pstride + off] = (TS)v.y;
+            } else {
+                planes[(long long)q * pstride + off] = (TS)v.x;
+                if (v.y != 0.0) *flag = 1;
+            }
+        } else {
+            const long long j = i - (long long)nh * pstride;
+            fields[j] = (TS)v.x;
+            if (v.y != 0.0) *flag = 1;
+        }
+    }
+}
+
+template <typename TS>
+__global__ void gather_kernel(double2* __restrict__ dst, const double* f00, const TS* planes, const TS* fields,
+                              const int* __restrict__ hplane, long long pstride, int nh, long long cells) {
+    const long long total = (long long)nh * pstride + 6 * cells;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        double2 v;
+        if (i < (long long)nh * pstride) {
+            const int h = (int)(i / pstride);
+            const long long off = i - (long long)h * pstride;
+            const int q = hplane[h];
+            if (q < 0) v = make_double2(f00[off], 0.0);
+            else if (hplane[nh + h]) v = make_double2((double)planes[(long long)q * pstride + off],
+                                                      (double)planes[(long long)(q + 1) * pstride + off]);
+            else v = make_double2((double)planes[(long long)q * pstride + off], 0.0);
+        } else {
+            v = make_double2((double)fields[i - (long long)nh * pstride], 0.0);
+        }
+        dst[i] = v;
+    }
+}
+
+__global__ void clock_advance_kernel(Clock* c, double dt) { c->t += dt; }
+__global__ void clock_commit_kernel(Clock* c, int ee, int eb) {
+    if (ee) c->t_ee = c->t;
+    if (eb) c->t_eb = c->t;
+}
+
+template <typename T>
+__global__ void nan_kernel(const T* x, long long n, int* status) {
+    bool bad = false;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (!isfinite((double)x[i])) bad = true;
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, 2);
+}
+
+int grid_for(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+}  // namespace
+
+cudaError_t launch_nan_check(const double* f00, const void* planes, int planes_fp32, long long n_f00,
+                             long long n_planes, const void* fields, long long n_fields, int* status,
+                             cudaStream_t s) {
+    nan_kernel<double><<<grid_for(n_f00, 256), 256, 0, s>>>(f00, n_f00, status);
+    if (planes_fp32) {
+        if (n_planes) nan_kernel<float><<<grid_for(n_planes, 256), 256, 0, s>>>((const float*)planes, n_planes, status);
+        nan_kernel<float><<<grid_for(n_fields, 256), 256, 0, s>>>((const float*)fields, n_fields, status);
+    } else {
+        if (n_planes) nan_kernel<double><<<grid_for(n_planes, 256), 256, 0, s>>>((const double*)planes, n_planes, status);
+        nan_kernel<double><<<grid_for(n_fields, 256), 256, 0, s>>>((const double*)fields, n_fields, status);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace oshun
+
+using namespace oshun;
+
+struct oshun_ctx {
+    oshun_cfg cfg;
+    int nh = 0, nplanes = 0, mc = 0;
+    long long cells = 0, pstride = 0;
+    bool fp32 = false;
+    size_t ts = 8;
+    int dev = 0;
+
+    double* f00[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* pl[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* fld[4] = {nullptr, nullptr, nullptr, nullptr};
+    int cur = 0;
+
+    CoefLM* d_coef = nullptr;
+    int* d_plane_of = nullptr;   // [(l0+1)*(m0+1)]
+    int* d_plane_l = nullptr;    // [nplanes]
+    int* d_plane_m = nullptr;    // [nplanes]
+    int* d_hplane = nullptr;     // [2*nh]: plane of Re (or -1 for f00), complex flag
+    double* d_ptab = nullptr;    // inv_pr, vr, wj
+    double* d_vtab = nullptr;    // vr, U4, U4m1, U2, U2m1, U1, U1m1, U3, Qn, Pn
+    double* d_dense_ws = nullptr;
+    int dense_blocks = 0;
+    int* d_status = nullptr;
+    Clock* d_clock = nullptr;
+    double2* d_stage = nullptr;  // host-layout staging for transfers and slopes
+
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][collisions]
+
+    // host mirrors of the clocks (the reference's Runge_Kutta_4::t, Explicit_EC_FP::t, Euler_Backward::t)
+    double t = 0.0, t_ee = 0.0, t_eb = 0.0;
+
+    int collide_chunk = 0;
+    size_t collide_smem = 0;
+    int collide_blocks = 0;
+
+    // constants
+    double dp = 0, idx = 0, idy = 0, g00_s = 0, g00_inv = 0, g00_gr = 0, c_kpre = 0, kpre = 0;
+
+    template <typename TS>
+    StageArgs<TS> stage_args(int in_set, int out_set, int mode) const;
+};
+
+namespace {
+
+#define CK(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));            \
+            return OSHUN_ERR_CUDA;                                                    \
+        }                                                                             \
+    } while (0)
+
+double axis_point(int i, int n, double lo, double hi) {
+    const double step = (hi - lo) / (double)(n - 1);
+    return (double)i * step + lo;
+}
+double local_dx(int nglob, double lo, double hi) {
+    const double dg = axis_point(1, nglob, lo, hi) - axis_point(0, nglob, lo, hi);
+    const double x0 = axis_point(0, nglob, lo, hi) - 4.0 * dg;
+    const double x1 = x0 + dg;
+    return x1 - x0;
+}
+
+int num_harmonics(int l0, int m0) { return ((m0 + 1) * (2 * l0 - m0 + 2)) / 2; }
+
+int ind(int l, int m, int m0) {
+    return (l < m0 + 1) ? (l * (l + 1)) / 2 + m : l * (m0 + 1) - (m0 * (m0 + 1)) / 2 + m;
+}
+
+const double kRe = 2.8179402894e-13;  // classical electron radius in cm (def-FokkerPlanck.cpp:136)
+
+// Reference y-advection chain factor for m >= 2 (OSHUN-1/def-VlasovMax.cpp:901-946):
+// the loop multiplier is divided by C1[m+1] where C1[l-1] is meant (line 918) and
+// carries into the next m.  Returned factor multiplies every y coupling of (l,m).
+double yadv_chain(int l, int m, int l0, int m0, double idy, bool keep) {
+    if (!keep || m < 2) return 1.0;
+    auto C1 = [&](int ll) { return (-0.5) * idy / (2.0 * ll + 1.0); };
+    double R = 1.0;
+    for (int mm = 2; mm <= m; ++mm) {
+        if (mm == m0) return R;
+        if (mm + 1 >= l0) {
+            if (mm == m) return R;
+            continue;
+        }
+        double q = R, at_l = R;
+        for (int ll = mm + 2; ll <= l0 - 1; ++ll) {
+            if (ll > mm + 2) q = q * (C1(ll - 1) / C1(mm + 1));
+            if (mm == m && ll == l) at_l = q;
+        }
+        if (mm == m) {
+            if (l <= mm + 1) return R;
+            if (l == l0) return q;
+            return at_l;
+        }
+        R = q;
+    }
+    return R;
+}
+
+int validate(const oshun_cfg* c) {
+    if (!c) { set_error("cfg is NULL"); return OSHUN_ERR_ARG; }
+    if (c->l0 < 1 || c->m0 < 0 || c->m0 > c->l0) { set_error("need 1 <= l0 and 0 <= m0 <= l0"); return OSHUN_ERR_ARG; }
+    if (c->m0 > kMaxM0) { set_error("m0 above the compiled maximum of 8"); return OSHUN_ERR_UNSUPPORTED; }
+    if (c->nump < 3 || c->nump > kMaxNp) { set_error("need 3 <= nump <= 1024"); return OSHUN_ERR_ARG; }
+    if (c->numx < 1 || c->numy < 1) { set_error("need numx, numy >= 1"); return OSHUN_ERR_ARG; }
+    if (c->numx < 2 && c->numy < 2) { set_error("need at least two cells"); return OSHUN_ERR_ARG; }
+    if (!(c->pmax > c->pmin) || !(c->pmin > 0.0)) { set_error("need 0 < pmin < pmax"); return OSHUN_ERR_ARG; }
+    if (!(c->xmax > c->xmin) || (c->numy > 1 && !(c->ymax > c->ymin))) { set_error("bad x/y extent"); return OSHUN_ERR_ARG; }
+    if (!(c->dt > 0.0) || !(c->small_dt > 0.0)) { set_error("need dt > 0 and small_dt > 0"); return OSHUN_ERR_ARG; }
+    if (!(c->density_np > 0.0)) { set_error("need density_np > 0"); return OSHUN_ERR_ARG; }
+    if (c->precision != OSHUN_FP64 && c->precision != OSHUN_FP32_SPLIT) { set_error("bad precision"); return OSHUN_ERR_ARG; }
+    return OSHUN_OK;
+}
+
+int pick_mc(int m0) {
+    const int caps[] = {0, 1, 2, 3, 4, 6, 8};
+    for (int c : caps)
+        if (c >= m0) return c;
+    return -1;
+}
+
+}  // namespace
+
+template <typename TS>
+StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
+    StageArgs<TS> a;
+    std::memset(&a, 0, sizeof(a));
+    a.f00_in = f00[in_set]; a.pl_in = (const TS*)pl[in_set]; a.fld_in = (const TS*)fld[in_set];
+    a.coef = d_coef; a.plane_of = d_plane_of;
+    a.inv_pr = d_ptab; a.vr = d_ptab + cfg.nump; a.wj = d_ptab + 2 * cfg.nump;
+    a.cells = cells; a.pstride = pstride;
+    a.np = cfg.nump; a.nx = cfg.numx; a.ny = cfg.numy; a.l0 = cfg.l0; a.m0 = cfg.m0;
+    a.mode = mode;
+    a.g00_s = g00_s; a.g00_inv = g00_inv; a.g00_gr = g00_gr;
+    a.idx = idx; a.idy = idy;
+    (void)out_set;
+    return a;
+}
+
+namespace {
+
+int build_tables(oshun_ctx* h) {
+    const oshun_cfg& c = h->cfg;
+    const int np = c.nump, l0 = c.l0, m0 = c.m0;
+    std::vector<double> pr(np), inv_pr(np), vr(np);
+    for (int i = 0; i < np; ++i) {
+        pr[i] = axis_point(i, np, c.pmin, c.pmax);
+        inv_pr[i] = 1.0 / pr[i];
+        vr[i] = pr[i] / std::sqrt(1.0 + pr[i] * pr[i]);
+    }
+    const double dp = pr[1] - pr[0];
+    h->dp = dp;
+    h->idx = -1.0 / (2.0 * local_dx(c.numx, c.xmin, c.xmax));
+    h->idy = c.numy > 1 ? -1.0 / (2.0 * local_dx(c.numy, c.ymin, c.ymax)) : 0.0;
+    const double p0 = pr[0], p1 = pr[1];
+    h->g00_s = p0 * p0 / (p1 * p1);
+    h->g00_inv = 1.0 / (1.0 - h->g00_s);
+    h->g00_gr = -4.0 * dp * p0 / (p1 * p1);
+
+    // current quadrature (Current ctor and Jxyz, def-VlasovMax.cpp:670-712)
+    std::vector<double> wj(np);
+    double small = p0;
+    small *= small; small *= small; small *= p0; small *= 0.2; small *= 1.0 / p1;
+    for (int i = 0; i < np; ++i) {
+        const double q = pr[i];
+        const double p3og = (q * q) * (q / std::sqrt(1.0 + q * q));
+        double w = (i == 0 || i == np - 1) ? 0.5 * dp * p3og : dp * p3og;
+        if (i == 1) w += small * p3og;
+        wj[i] = w * (4.0 * M_PI / 3.0);
+    }
+
+    // coupling tables
+    const bool keep_chain = !(c.flags & OSHUN_FLAG_FIX_YADV_CHAIN);
+    std::vector<CoefLM> coef((size_t)(l0 + 1) * (m0 + 1));
+    std::memset(coef.data(), 0, sizeof(CoefLM) * coef.size());
+    auto exists = [&](int l, int m) { return l >= 0 && l <= l0 && m >= 0 && m <= m0 && m <= l; };
+    const double hdp = 0.5 / dp, qdp = 0.25 / dp;
+    for (int l = 0; l <= l0; ++l)
+        for (int m = 0; m <= std::min(l, m0); ++m) {
+            CoefLM& k = coef[(size_t)l * (m0 + 1) + m];
+            const double L = l, M = m;
+            // E field (ElectricField ctor, def-VlasovMax.cpp:97-140)
+            const double A1 = (l == 0) ? -1.0 * hdp : (L + 1.0 - M) * L / ((2.0 * L + 1.0) * (L + 1.0)) * hdp;
+            const double A2 = -(L + M) / (2.0 * L + 1.0) * hdp;
+            const double C1 = (l == 0) ? -qdp : qdp * L / ((2.0 * L + 1.0) * (L + 1.0));
+            const double C3 = qdp / (2.0 * L + 1.0);
+            const double B1 = (-hdp) * L * L / (2.0 * L + 1.0);
+            const double B2 = (-hdp) * L * (L + 1.0) / (2.0 * L + 1.0);
+            const double C2 = (-qdp) * L * (L - M + 2.0) * (L - M + 1.0) / ((2.0 * L + 1.0) * (L + 1.0));
+            const double C4 = (-qdp) * (L + M - 1.0) * (L + M) / (2.0 * L + 1.0);
+            k.ex_g = exists(l + 1, m) ? A1 : 0.0;
+            k.ex_h = exists(l - 1, m) ? A2 : 0.0;
+            k.em_g = exists(l + 1, m + 1) ? C1 : 0.0;
+            k.em_h = exists(l - 1, m + 1) ? C3 : 0.0;
+            if (m == 1) {
+                k.ep_h = exists(l - 1, 0) ? B2 : 0.0;
+                k.ep_g = exists(l + 1, 0) ? B1 : 0.0;
+            } else if (m >= 2) {
+                k.ep_h = exists(l - 1, m - 1) ? C4 : 0.0;
+                k.ep_g = exists(l + 1, m - 1) ? C2 : 0.0;
+            }
+            // advection (Spatial_Advection ctor, def-VlasovMax.cpp:775-826)
+            const double ix = h->idx, iy = h->idy;
+            k.ax_p = exists(l + 1, m) ? ix * (-1.0) * (L - M + 1.0) / (2.0 * L + 1.0) : 0.0;
+            k.ax_m = exists(l - 1, m) ? ix * (-1.0) * (L + M) / (2.0 * L + 1.0) : 0.0;
+            if (c.numy > 1) {
+                const double q = yadv_chain(l, m, l0, m0, iy, keep_chain);
+                const double yC1 = (-0.5) * iy / (2.0 * L + 1.0);
+                const double yC3 = -yC1;
+                const double yB1 = iy * (L + 1.0) * L / (2.0 * L + 1.0);
+                const double yB2 = -yB1;
+                const double yC2 = iy * 0.5 * (L + 2.0 - M) * (L - M + 1.0) / (2.0 * L + 1.0);
+                const double yC4 = iy * (-0.5) * (L + M - 1.0) * (L + M) / (2.0 * L + 1.0);
+                k.ay_pp = exists(l + 1, m + 1) ? q * yC1 : 0.0;
+                k.ay_mp = exists(l - 1, m + 1) ? q * yC3 : 0.0;
+                if (m == 1) {
+                    k.ay_mm = exists(l - 1, 0) ? yB2 : 0.0;
+                    k.ay_pm = exists(l + 1, 0) ? yB1 : 0.0;
+                } else if (m >= 2) {
+                    k.ay_mm = exists(l - 1, m - 1) ? q * yC4 : 0.0;
+                    k.ay_pm = exists(l + 1, m - 1) ? q * yC2 : 0.0;
+                }
+            }
+            // B field (MagneticField ctor, def-VlasovMax.cpp:563-589)
+            if (m == 1) k.b_m = -L * (L + 1.0);
+            else if (m >= 2) k.b_m = (-0.5) * (L + 1.0 - M) * (L + M);
+            // G/H (MakeGH, def-VlasovMax.cpp:496-515; Hp0, :145-147)
+            if (l >= 1) {
+                k.gfac = -(2.0 * L + 1.0) / L;
+                k.invpax = -2.0 * (L + 1.0) * dp;
+                double hp = 1.0 / p0;
+                for (int kk = 1; kk <= l; ++kk) hp = hp * (p0 / p1) * (2.0 * kk + 1.0) / (2.0 * kk - 1);
+                k.hp0 = hp * (-2.0 * dp);
+            }
+        }
+
+    // plane maps
+    std::vector<int> plane_of((size_t)(l0 + 1) * (m0 + 1), -1), plane_l, plane_m;
+    std::vector<int> hplane(2 * (size_t)h->nh, 0);
+    int q = 0;
+    for (int l = 0; l <= l0; ++l)
+        for (int m = 0; m <= std::min(l, m0); ++m) {
+            const int hi = ind(l, m, m0);
+            if (l == 0) { hplane[hi] = -1; continue; }
+            plane_of[(size_t)l * (m0 + 1) + m] = q;
+            hplane[hi] = q;
+            hplane[h->nh + hi] = m > 0 ? 1 : 0;
+            const int ncomp = m > 0 ? 2 : 1;
+            for (int k = 0; k < ncomp; ++k) { plane_l.push_back(l); plane_m.push_back(m); }
+            q += ncomp;
+        }
+    h->nplanes = q;
+
+    // velocity grid of the collision operators (def-FokkerPlanck.cpp:143-172, 790-803)
+    std::vector<double> vt((size_t)10 * np, 0.0);
+    double* V = vt.data();
+    for (int i = 0; i < np; ++i) V[i] = vr[i];
+    for (int i = 1; i < np; ++i) {
+        const double dv = vr[i] - vr[i - 1];
+        V[np + i] = 0.5 * std::pow(vr[i], 4) * dv;
+        V[2 * np + i] = 0.5 * std::pow(vr[i - 1], 4) * dv;
+        V[3 * np + i] = 0.5 * vr[i] * vr[i] * dv;
+        V[4 * np + i] = 0.5 * vr[i - 1] * vr[i - 1] * dv;
+        V[5 * np + i] = 0.5 * vr[i] * dv;
+        V[6 * np + i] = 0.5 * vr[i - 1] * dv;
+    }
+    for (int i = 0; i < np; ++i) V[7 * np + i] = std::pow(vr[i], 3);
+    V[8 * np + 0] = 1.0 / ((vr[0] * vr[0] * vr[1]) / 2.0);
+    for (int i = 1; i < np - 1; ++i) V[8 * np + i] = 1.0 / (vr[i] * vr[i] * (vr[i + 1] - vr[i - 1]) / 2.0);
+    for (int i = 0; i < np - 1; ++i) V[9 * np + i] = 1.0 / ((vr[i + 1] - vr[i]) / 2.0 * (vr[i + 1] + vr[i]));
+    const double kp = std::sqrt(4.0 * M_PI * c.density_np * kRe);
+    h->c_kpre = 4.0 * M_PI / 3.0 * kRe * kp;
+    h->kpre = kRe * kp;
+
+    std::vector<double> ptab((size_t)3 * np);
+    for (int i = 0; i < np; ++i) { ptab[i] = inv_pr[i]; ptab[np + i] = vr[i]; ptab[2 * np + i] = wj[i]; }
+
+    CK(cudaMalloc(&h->d_coef, sizeof(CoefLM) * coef.size()));
+    CK(cudaMemcpy(h->d_coef, coef.data(), sizeof(CoefLM) * coef.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_plane_of, sizeof(int) * plane_of.size()));
+    CK(cudaMemcpy(h->d_plane_of, plane_of.data(), sizeof(int) * plane_of.size(), cudaMemcpyHostToDevice));
+    const size_t npl = std::max<size_t>(1, plane_l.size());
+    CK(cudaMalloc(&h->d_plane_l, sizeof(int) * npl));
+    CK(cudaMalloc(&h->d_plane_m, sizeof(int) * npl));
+    if (!plane_l.empty()) {
+        CK(cudaMemcpy(h->d_plane_l, plane_l.data(), sizeof(int) * plane_l.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->d_plane_m, plane_m.data(), sizeof(int) * plane_m.size(), cudaMemcpyHostToDevice));
+    }
+    CK(cudaMalloc(&h->d_hplane, sizeof(int) * hplane.size()));
+    CK(cudaMemcpy(h->d_hplane, hplane.data(), sizeof(int) * hplane.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_ptab, sizeof(double) * ptab.size()));
+    CK(cudaMemcpy(h->d_ptab, ptab.data(), sizeof(double) * ptab.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_vtab, sizeof(double) * vt.size()));
+    CK(cudaMemcpy(h->d_vtab, vt.data(), sizeof(double) * vt.size(), cudaMemcpyHostToDevice));
+    return OSHUN_OK;
+}
+
+int launch_stage(oshun_ctx* h, int in_set, int B_set, int A_set, int out_set, int mode, int first, double c1,
+                 double c2) {
+    cudaError_t e;
+    if (h->fp32) {
+        StageArgs<float> a = h->stage_args<float>(in_set, out_set, mode);
+        a.f00_B = h->f00[B_set]; a.pl_B = (const float*)h->pl[B_set]; a.fld_B = (const float*)h->fld[B_set];
+        a.f00_A = h->f00[A_set]; a.pl_A = (float*)h->pl[A_set]; a.fld_A = (float*)h->fld[A_set];
+        if (out_set >= 0) { a.f00_out = h->f00[out_set]; a.pl_out = (float*)h->pl[out_set]; a.fld_out = (float*)h->fld[out_set]; }
+        a.first = first; a.c1 = c1; a.c2 = c2;
+        e = launch_stage_fp32(a, h->mc, h->stream);
+    } else {
+        StageArgs<double> a = h->stage_args<double>(in_set, out_set, mode);
+        a.f00_B = h->f00[B_set]; a.pl_B = (const double*)h->pl[B_set]; a.fld_B = (const double*)h->fld[B_set];
+        a.f00_A = h->f00[A_set]; a.pl_A = (double*)h->pl[A_set]; a.fld_A = (double*)h->fld[A_set];
+        if (out_set >= 0) { a.f00_out = h->f00[out_set]; a.pl_out = (double*)h->pl[out_set]; a.fld_out = (double*)h->fld[out_set]; }
+        a.first = first; a.c1 = c1; a.c2 = c2;
+        e = launch_stage_fp64(a, h->mc, h->stream);
+    }
+    if (e != cudaSuccess) { set_error(std::string("rk stage launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+    return OSHUN_OK;
+}
+
+// Runge_Kutta_4::advance_p1 (def-RK.cpp:116-142) on set cur -> set nxt
+int enqueue_rk4(oshun_ctx* h) {
+    const double dt = h->cfg.dt;
+    const int B = h->cur, A = h->cur ^ 1, Sa = 2, Sb = 3;
+    int rc;
+    if ((rc = launch_stage(h, B, B, A, Sa, 0, 1, 0.5 * dt, 1.0 / 3.0))) return rc;   // k1
+    if ((rc = launch_stage(h, Sa, B, A, Sb, 0, 0, 0.5 * dt, 2.0 / 3.0))) return rc;  // k2
+    if ((rc = launch_stage(h, Sb, B, A, Sa, 0, 0, dt, 1.0 / 3.0))) return rc;        // k3
+    if ((rc = launch_stage(h, Sa, B, A, -1, 0, 0, dt / 6.0, 1.0))) return rc;         // k4
+    return OSHUN_OK;
+}
+
+CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt) {
+    CollideArgs a;
+    std::memset(&a, 0, sizeof(a));
+    const oshun_cfg& c = h->cfg;
+    const int np = c.nump;
+    a.f00 = h->f00[h->cur];
+    a.planes = h->pl[h->cur];
+    a.planes_fp32 = h->fp32 ? 1 : 0;
+    a.plane_of = h->d_plane_of; a.plane_l = h->d_plane_l; a.plane_m = h->d_plane_m;
+    a.nplanes = h->nplanes;
+    a.cells = h->cells; a.pstride = h->pstride;
+    a.np = np; a.l0 = c.l0; a.m0 = c.m0;
+    a.mmax_coll = c.if_implicit1D ? 0 : c.m0;
+    a.do_ee = do_ee; a.do_l1 = do_l1; a.do_lm = do_lm;
+    a.if_tridiagonal = c.if_tridiagonal;
+    a.nsub = nsub; a.hsub = hsub; a.Dt = Dt;
+    a.NB = c.NB_algorithms;
+    a.density_np = c.density_np; a.Zeta = c.Zeta;
+    a.c_kpre = h->c_kpre; a.kpre = h->kpre;
+    const double* V = h->d_vtab;
+    a.vr = V; a.U4 = V + np; a.U4m1 = V + 2 * np; a.U2 = V + 3 * np; a.U2m1 = V + 4 * np;
+    a.U1 = V + 5 * np; a.U1m1 = V + 6 * np; a.U3 = V + 7 * np; a.Qn = V + 8 * np; a.Pn = V + 9 * np;
+    a.chunk = h->collide_chunk;
+    a.dense_ws = h->d_dense_ws;
+    a.status = h->d_status;
+    return a;
+}
+
+int enqueue_collide(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt) {
+    CollideArgs a = collide_args(h, do_ee, do_l1, do_lm, nsub, hsub, Dt);
+    cudaError_t e = launch_collide(a, h->stream, h->collide_smem, h->collide_blocks);
+    if (e != cudaSuccess) { set_error(std::string("collide launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+    return OSHUN_OK;
+}
+
+// the reference's clock arithmetic for one small step ending at t_new
+void collide_params(const oshun_ctx* h, double t_new, int* nsub, double* hsub, double* Dt) {
+    *nsub = (int)((t_new - h->t_ee) / h->cfg.small_dt) + 1;   // def-FokkerPlanck.cpp:598-599
+    *hsub = (t_new - h->t_ee) / (double)(*nsub);
+    *Dt = t_new - h->t_eb;                                     // def-FokkerPlanck.cpp:1277,1297
+}
+
+void free_ctx(oshun_ctx* h) {
+    for (int p = 0; p < 2; ++p)
+        for (int c = 0; c < 2; ++c)
+            if (h->graph[p][c]) cudaGraphExecDestroy(h->graph[p][c]);
+    for (int i = 0; i < 4; ++i) { cudaFree(h->f00[i]); cudaFree(h->pl[i]); cudaFree(h->fld[i]); }
+    cudaFree(h->d_coef); cudaFree(h->d_plane_of); cudaFree(h->d_plane_l); cudaFree(h->d_plane_m);
+    cudaFree(h->d_hplane); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
+    cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oshun_abi_version(void) { return OSHUN_ABI_VERSION; }
+const char* oshun_last_error(void) { return g_last_error.c_str(); }
+
+int oshun_create(const oshun_cfg* cfg, oshun_handle* out) {
+    if (!out) { set_error("out is NULL"); return OSHUN_ERR_ARG; }
+    *out = nullptr;
+    int rc = validate(cfg);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) { set_error("no CUDA device"); return OSHUN_ERR_NO_DEVICE; }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) { set_error("liboshun_b200 is built for sm_100a (B200)"); return OSHUN_ERR_NO_DEVICE; }
+
+    oshun_ctx* h = new oshun_ctx();
+    h->cfg = *cfg;
+    h->dev = dev;
+    h->nh = num_harmonics(cfg->l0, cfg->m0);
+    h->mc = pick_mc(cfg->m0);
+    h->cells = (long long)cfg->numx * cfg->numy;
+    h->pstride = h->cells * cfg->nump;
+    h->fp32 = cfg->precision == OSHUN_FP32_SPLIT;
+    h->ts = h->fp32 ? 4 : 8;
+    h->t = h->t_ee = h->t_eb = cfg->t0;
+    auto fail = [&](int code) { free_ctx(h); return code; };
+#define CKF(call)                                                                  \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+            return fail(OSHUN_ERR_CUDA);                                           \
+        }                                                                          \
+    } while (0)
+    if ((rc = build_tables(h))) return fail(rc);
+    for (int i = 0; i < 4; ++i) {
+        CKF(cudaMalloc(&h->f00[i], sizeof(double) * h->pstride));
+        CKF(cudaMalloc(&h->pl[i], h->ts * std::max<long long>(1, (long long)h->nplanes * h->pstride)));
+        CKF(cudaMalloc(&h->fld[i], h->ts * 6 * h->cells));
+        CKF(cudaMemset(h->f00[i], 0, sizeof(double) * h->pstride));
+        CKF(cudaMemset(h->pl[i], 0, h->ts * std::max<long long>(1, (long long)h->nplanes * h->pstride)));
+        CKF(cudaMemset(h->fld[i], 0, h->ts * 6 * h->cells));
+    }
+    CKF(cudaMalloc(&h->d_status, sizeof(int) * 4));
+    CKF(cudaMemset(h->d_status, 0, sizeof(int) * 4));
+    CKF(cudaMalloc(&h->d_clock, sizeof(Clock)));
+    Clock ck{h->t, h->t_ee, h->t_eb};
+    CKF(cudaMemcpy(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice));
+    CKF(cudaMalloc(&h->d_stage, sizeof(double2) * ((size_t)h->nh * h->pstride + 6 * h->cells)));
+    CKF(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+
+    // collision launch shape
+    const int np = cfg->nump;
+    int smem_optin = 0;
+    CKF(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t budget = std::min<size_t>((size_t)smem_optin, 200 * 1024);
+    if (cfg->if_tridiagonal) {
+        int chunk = collide_max_chunk(np, budget);
+        if (chunk < 1) { set_error("nump too large for the collision kernel's shared memory"); return fail(OSHUN_ERR_UNSUPPORTED); }
+        chunk = std::min(chunk, std::max(1, h->nplanes));
+        h->collide_chunk = chunk;
+        h->collide_smem = collide_smem_bytes(np, chunk, 1);
+        h->collide_blocks = (int)std::min<long long>(h->cells, (long long)prop.multiProcessorCount * 16);
+    } else {
+        h->collide_smem = collide_smem_bytes(np, 0, 0);
+        if (h->collide_smem > budget) { set_error("nump too large for the dense collision path"); return fail(OSHUN_ERR_UNSUPPORTED); }
+        h->collide_blocks = (int)std::min<long long>(h->cells, (long long)prop.multiProcessorCount * 4);
+        h->dense_blocks = h->collide_blocks;
+        CKF(cudaMalloc(&h->d_dense_ws, sizeof(double) * (size_t)np * np * h->dense_blocks));
+    }
+#undef CKF
+    *out = h;
+    return OSHUN_OK;
+}
+
+int oshun_destroy(oshun_handle h) {
+    if (!h) return OSHUN_ERR_ARG;
+    cudaStreamSynchronize(h->stream);
+    free_ctx(h);
+    return OSHUN_OK;
+}
+
+int oshun_set_stream(oshun_handle h, void* stream) {
+    if (!h) return OSHUN_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->own_stream) { cudaStreamDestroy(h->stream); h->own_stream = false; }
+    for (int p = 0; p < 2; ++p)
+        for (int c = 0; c < 2; ++c)
+            if (h->graph[p][c]) { cudaGraphExecDestroy(h->graph[p][c]); h->graph[p][c] = nullptr; }
+    if (stream) {
+        h->stream = (cudaStream_t)stream;
+    } else {
+        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->own_stream = true;
+    }
+    return OSHUN_OK;
+}
+
+int oshun_synchronize(oshun_handle h) {
+    if (!h) return OSHUN_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_upload(oshun_handle h, const double* harmonics, const double* fields) {
+    if (!h || !harmonics || !fields) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    const size_t nb_h = sizeof(double2) * (size_t)h->nh * h->pstride;
+    const size_t nb_f = sizeof(double2) * 6 * (size_t)h->cells;
+    CK(cudaMemcpyAsync(h->d_stage, harmonics, nb_h, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync((char*)h->d_stage + nb_h, fields, nb_f, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->d_status + 2, 0, sizeof(int), h->stream));
+    const long long total = (long long)h->nh * h->pstride + 6 * h->cells;
+    const int set = h->cur;
+    if (h->fp32)
+        scatter_kernel<float><<<grid_for(total, 256), 256, 0, h->stream>>>(
+            h->d_stage, h->f00[set], (float*)h->pl[set], (float*)h->fld[set], h->d_hplane, h->pstride, h->nh,
+            h->cells, h->d_status + 2);
+    else
+        scatter_kernel<double><<<grid_for(total, 256), 256, 0, h->stream>>>(
+            h->d_stage, h->f00[set], (double*)h->pl[set], (double*)h->fld[set], h->d_hplane, h->pstride, h->nh,
+            h->cells, h->d_status + 2);
+    CK(cudaGetLastError());
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, h->d_status + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (flag) { set_error("an m=0 harmonic or a field has a nonzero imaginary part"); return OSHUN_ERR_NONREAL; }
+    return OSHUN_OK;
+}
+
+static int gather_to_host(oshun_handle h, int set, double* harmonics, double* fields) {
+    const long long total = (long long)h->nh * h->pstride + 6 * h->cells;
+    if (h->fp32)
+        gather_kernel<float><<<grid_for(total, 256), 256, 0, h->stream>>>(
+            h->d_stage, h->f00[set], (const float*)h->pl[set], (const float*)h->fld[set], h->d_hplane, h->pstride,
+            h->nh, h->cells);
+    else
+        gather_kernel<double><<<grid_for(total, 256), 256, 0, h->stream>>>(
+            h->d_stage, h->f00[set], (const double*)h->pl[set], (const double*)h->fld[set], h->d_hplane,
+            h->pstride, h->nh, h->cells);
+    CK(cudaGetLastError());
+    const size_t nb_h = sizeof(double2) * (size_t)h->nh * h->pstride;
+    const size_t nb_f = sizeof(double2) * 6 * (size_t)h->cells;
+    CK(cudaMemcpyAsync(harmonics, h->d_stage, nb_h, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(fields, (char*)h->d_stage + nb_h, nb_f, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_download(oshun_handle h, double* harmonics, double* fields) {
+    if (!h || !harmonics || !fields) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    return gather_to_host(h, h->cur, harmonics, fields);
+}
+
+int oshun_rhs(oshun_handle h, double* slope_harmonics, double* slope_fields) {
+    if (!h || !slope_harmonics || !slope_fields) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    // slope written to set 2 (scratch), in plane layout
+    int rc = launch_stage(h, h->cur, h->cur, h->cur, 2, 1, 0, 1.0, 1.0);
+    if (rc) return rc;
+    return gather_to_host(h, 2, slope_harmonics, slope_fields);
+}
+
+int oshun_rk4_step(oshun_handle h) {
+    if (!h) return OSHUN_ERR_ARG;
+    int rc = enqueue_rk4(h);
+    if (rc) return rc;
+    h->cur ^= 1;
+    h->t += h->cfg.dt;
+    clock_advance_kernel<<<1, 1, 0, h->stream>>>(h->d_clock, h->cfg.dt);
+    CK(cudaGetLastError());
+    return OSHUN_OK;
+}
+
+int oshun_collide_ee(oshun_handle h, double t_new) {
+    if (!h) return OSHUN_ERR_ARG;
+    int nsub; double hsub, Dt;
+    collide_params(h, t_new, &nsub, &hsub, &Dt);
+    int rc = enqueue_collide(h, 1, 0, 0, nsub, hsub, Dt);
+    if (rc) return rc;
+    h->t_ee = t_new;
+    Clock ck{h->t, h->t_ee, h->t_eb};
+    CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_collide_f1(oshun_handle h, double t_new) {
+    if (!h) return OSHUN_ERR_ARG;
+    int nsub; double hsub, Dt;
+    collide_params(h, t_new, &nsub, &hsub, &Dt);
+    return enqueue_collide(h, 0, 1, 0, nsub, hsub, Dt);
+}
+
+int oshun_collide_flm(oshun_handle h, double t_new) {
+    if (!h) return OSHUN_ERR_ARG;
+    int nsub; double hsub, Dt;
+    collide_params(h, t_new, &nsub, &hsub, &Dt);
+    int rc = enqueue_collide(h, 0, 0, 1, nsub, hsub, Dt);
+    if (rc) return rc;
+    h->t_eb = t_new;
+    Clock ck{h->t, h->t_ee, h->t_eb};
+    CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_step(oshun_handle h, int nsteps, int collisions) {
+    if (!h || nsteps < 0) return OSHUN_ERR_ARG;
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = enqueue_rk4(h);
+        if (rc) return rc;
+        h->cur ^= 1;
+        h->t += h->cfg.dt;
+        if (collisions) {
+            int nsub; double hsub, Dt;
+            collide_params(h, h->t, &nsub, &hsub, &Dt);
+            rc = enqueue_collide(h, 1, 1, 1, nsub, hsub, Dt);
+            if (rc) return rc;
+            h->t_ee = h->t;
+            h->t_eb = h->t;
+        }
+    }
+    Clock ck{h->t, h->t_ee, h->t_eb};
+    CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_time(oshun_handle h, double* t) {
+    if (!h || !t) return OSHUN_ERR_ARG;
+    *t = h->t;
+    return OSHUN_OK;
+}
+
+int oshun_status_flags(oshun_handle h, int* flags, long long* count) {
+    if (!h) return OSHUN_ERR_ARG;
+    const long long nf = h->pstride, npl = (long long)h->nplanes * h->pstride, nfl = 6 * h->cells;
+    CK(launch_nan_check(h->f00[h->cur], h->pl[h->cur], h->fp32, nf, npl, h->fld[h->cur], nfl, h->d_status, h->stream));
+    int st[2] = {0, 0};
+    CK(cudaMemcpyAsync(st, h->d_status, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * 2, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (flags) *flags = st[0];
+    if (count) *count = st[1];
+    return OSHUN_OK;
+}
+
+int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields, size_t* planes_bytes,
+                       size_t* fields_bytes) {
+    if (!h) return OSHUN_ERR_ARG;
+    if (f00) *f00 = h->f00[h->cur];
+    if (planes) *planes = h->pl[h->cur];
+    if (fields) *fields = h->fld[h->cur];
+    if (planes_bytes) *planes_bytes = h->ts * (size_t)h->nplanes * h->pstride;
+    if (fields_bytes) *fields_bytes = h->ts * 6 * (size_t)h->cells;
+    return OSHUN_OK;
+}
+
+int oshun_plane_index(oshun_handle h, int l, int m, int* plane) {
+    if (!h || !plane || l < 0 || l > h->cfg.l0 || m < 0 || m > h->cfg.m0 || m > l) return OSHUN_ERR_ARG;
+    if (l == 0) { *plane = -1; return OSHUN_OK; }
+    int q = 0;
+    for (int ll = 1; ll <= h->cfg.l0; ++ll)
+        for (int mm = 0; mm <= std::min(ll, h->cfg.m0); ++mm) {
+            if (ll == l && mm == m) { *plane = q; return OSHUN_OK; }
+            q += mm > 0 ? 2 : 1;
+        }
+    return OSHUN_ERR_ARG;
+}
+
+}  // extern "C"

@@ -1,0 +1,528 @@
+// Fokker-Planck collision step, one CTA per configuration-space cell
+// (grid-stride over cells), all arithmetic in FP64:
+//
+//   1. f00 e-e, Explicit_EC_FP::loop (OSHUN-1/def-FokkerPlanck.cpp:590-625):
+//      nsub RK4 substeps (RungeKutta4_ee::advance, :518-553) of Bell's
+//      number/energy conserving operator (EE_isotropic_conserva::Getslope,
+//      :192-267).  Warp 0 runs it; the cumulative integrals I4, I2 (forward)
+//      and J1 (backward) are warp scans over lane-owned runs of the p axis.
+//   2. Coefficients of the implicit f_lm step from the new f00,
+//      Implicit_FLM_step::reset_coeff (:808-939): I2, I0, J_{-1} scans,
+//      Coulomb logarithms, scattering term, the tridiagonal Alpha_Tri,
+//      f00 derivatives.  Computed once per cell for every l (the reference
+//      computes them in both f1_loop and flm_loop with the same f00).
+//   3. (I - Dt C_l) f_lm^{n+1} = f_lm^n for every collided plane,
+//      Implicit_FLM_step::advance (:943-1035):
+//      tridiagonal: the cell's planes are staged through shared memory in
+//        chunks and each thread runs the reference's Thomas recursion
+//        (TridiagonalSolve, OSHUN-1/def-Nmethods.cpp:142-167) on one plane;
+//      dense: per l the np x np matrix is assembled in a per-CTA global
+//        workspace and each warp runs the reference's Gauss-Seidel
+//        (def-Nmethods.cpp:44-136: dominance test, <= 5 sweeps, prefix
+//        convergence rule) on one complex right-hand side.
+#include <float.h>
+
+#include "oshun_internal.h"
+
+namespace oshun {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kCollideThreads = 128;
+
+// forward cumulative sum: out[k] = sum_{i=1..k} term(i), out[0] = 0
+template <class F>
+__device__ void warp_cumsum_fwd(double* out, int n, F term) {
+    const int lane = threadIdx.x & 31;
+    const int E = (n + 31) >> 5;
+    const int b = min(lane * E, n), e = min(b + E, n);
+    double loc = 0.0;
+    for (int k = b; k < e; ++k)
+        if (k > 0) loc += term(k);
+    double incl = loc;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double v = __shfl_up_sync(kFull, incl, off);
+        if (lane >= off) incl += v;
+    }
+    double run = __shfl_up_sync(kFull, incl, 1);
+    if (lane == 0) run = 0.0;
+    for (int k = b; k < e; ++k) {
+        if (k > 0) run += term(k);
+        out[k] = run;
+    }
+    __syncwarp();
+}
+
+// backward cumulative sum: out[k] = sum_{i=k+1..n-1} term(i), out[n-1] = 0
+template <class F>
+__device__ void warp_cumsum_bwd(double* out, int n, F term) {
+    const int lane = threadIdx.x & 31;
+    const int E = (n + 31) >> 5;
+    const int b = min(lane * E, n), e = min(b + E, n);
+    double loc = 0.0;
+    for (int i = b + 1; i <= e && i <= n - 1; ++i) loc += term(i);
+    double incl = loc;  // suffix sum over lanes >= lane
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double v = __shfl_down_sync(kFull, incl, off);
+        if (lane + off < 32) incl += v;
+    }
+    double run = __shfl_down_sync(kFull, incl, 1);
+    if (lane == 31) run = 0.0;
+    for (int k = e - 1; k >= b; --k) {
+        if (k + 1 <= n - 1) run += term(k + 1);
+        out[k] = run;
+    }
+    __syncwarp();
+}
+
+// Coulomb logarithms, NRL formulary as coded in OSHUN-1/def-FokkerPlanck.cpp:41-95
+__device__ double log_ee(double ne, double Te, double density_np) {
+    if (ne > 0.000000001) {
+        Te /= (3.0 * ne);
+        Te *= 511000;
+        ne *= density_np;
+        Te = log(Te);
+        ne = log(ne);
+        const double v = 23.5 - 0.5 * ne + 1.25 * Te - sqrt(0.00001 + 0.0625 * (Te - 2.0) * (Te - 2.0));
+        if (v > 2.0) return v;
+    }
+    return 2.0;
+}
+__device__ double zlog_ei(double ne, double Te, double density_np, double Zeta) {
+    if (ne > 0.0000001) {
+        Te /= (3.0 * ne);
+        Te *= 511000;
+        ne *= density_np;
+        Te = log(Te);
+        ne = log(ne);
+        const double v = 24.0 - 0.5 * ne + Te;
+        if (v > 2.0) return v * Zeta;
+    }
+    return 2.0 * Zeta;
+}
+
+struct Smem {
+    double *f, *f0, *f1, *fh, *I4, *I2, *J1;            // e-e work (np each)
+    double *tri_a, *tri_b, *tri_c, *scat, *df0, *ddf0;  // implicit coefficients (np each)
+    double* sc;                                          // scalars: [0] dense-term scale
+    double* chunk;                                       // staged planes / solver scratch
+};
+
+constexpr int kSmemArrays = 13;
+constexpr int kSmemScalars = 4;
+
+__device__ Smem carve(double* base, int np) {
+    Smem s;
+    s.f = base; s.f0 = base + np; s.f1 = base + 2 * np; s.fh = base + 3 * np;
+    s.I4 = base + 4 * np; s.I2 = base + 5 * np; s.J1 = base + 6 * np;
+    s.tri_a = base + 7 * np; s.tri_b = base + 8 * np; s.tri_c = base + 9 * np;
+    s.scat = base + 10 * np; s.df0 = base + 11 * np; s.ddf0 = base + 12 * np;
+    s.sc = base + kSmemArrays * np;
+    s.chunk = s.sc + kSmemScalars;
+    return s;
+}
+
+// EE_isotropic_conserva::Getslope on warp 0: fh = C_ee(fin)
+__device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin, double* fh) {
+    const int n = a.np;
+    const int lane = threadIdx.x & 31;
+    warp_cumsum_fwd(s.I4, n, [&](int k) { return a.U4[k] * fin[k] + a.U4m1[k] * fin[k - 1]; });
+    warp_cumsum_fwd(s.I2, n, [&](int k) { return a.U2[k] * fin[k] + a.U2m1[k] * fin[k - 1]; });
+    warp_cumsum_bwd(s.J1, n, [&](int i) { return a.U1[i] * fin[i] + a.U1m1[i] * fin[i - 1]; });
+    const double lnee = log_ee(4.0 * M_PI * s.I2[n - 1], 4.0 * M_PI * s.I4[n - 1], a.density_np);
+    const double* vr = a.vr;
+    const double v0s = vr[0] * vr[0], v1s = vr[1] * vr[1];
+    // flux G_n (stored in I4); the first NB cells use the parabolic fit near v = 0
+    for (int k = lane; k < n; k += 32) {
+        double g;
+        if (k < a.NB) {
+            const double f00 = (fin[0] - fin[1] * v0s / v1s) / (1.0 - v0s / v1s);
+            const double i2s = f00 * pow(vr[k], 3) / 3.0 + (fin[1] - f00) * pow(vr[k], 5) / v1s * 0.2;
+            const double i4s = f00 * pow(vr[k], 5) * 0.2 + (fin[1] - f00) * pow(vr[k], 7) / (v1s * 7.0);
+            g = fin[k] * i4s + (pow(vr[k], 3) * fin[k] - 3.0 * i2s) * s.J1[k];
+        } else {
+            double i2 = s.I2[k] * s.J1[k];
+            i2 *= -3.0;
+            double i4 = s.I4[k] + a.U3[k] * s.J1[k];
+            i4 *= fin[k];
+            g = i4 + i2;
+        }
+        s.I4[k] = g;
+    }
+    __syncwarp();
+    // D_k = (G_k - G_{k+1}) P_k for k < n-1, D_{n-1} = G_{n-1}   (kept in I2)
+    for (int k = lane; k < n; k += 32) s.I2[k] = (k < n - 1) ? (s.I4[k] - s.I4[k + 1]) * a.Pn[k] : s.I4[k];
+    __syncwarp();
+    const double norm = a.c_kpre * lnee;
+    for (int k = lane; k < n; k += 32) {
+        double v;
+        if (k == 0) {
+            v = (-1.0) * s.I4[0];
+            v *= 2.0 / v0s;
+            v -= s.I2[0];
+            v *= a.Qn[0];
+        } else {
+            v = a.Qn[k] * (s.I2[k - 1] - s.I2[k]);
+        }
+        fh[k] = v * norm;
+    }
+    __syncwarp();
+}
+
+// Implicit_FLM_step::reset_coeff on warp 0 (f = f00 of the cell in smem)
+__device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) {
+    const int n = a.np;
+    const int lane = threadIdx.x & 31;
+    const double* vr = a.vr;
+    double* I2 = s.I4;   // reuse the e-e work arrays
+    double* I0 = s.I2;
+    double* J1m = s.J1;
+    warp_cumsum_fwd(I2, n, [&](int k) { return a.U4[k] * f[k] + a.U4m1[k] * f[k - 1]; });
+    warp_cumsum_fwd(I0, n, [&](int k) { return a.U2[k] * f[k] + a.U2m1[k] * f[k - 1]; });
+    warp_cumsum_bwd(J1m, n, [&](int i) { return a.U1[i] * f[i] + a.U1m1[i] * f[i - 1]; });
+    const double I2_temperature = I2[n - 1] * (4.0 * M_PI);
+    const double I0_density = I0[n - 1] * (4.0 * M_PI);
+    const double lnee = log_ee(I0_density, I2_temperature, a.density_np);
+    const double zlnei = zlog_ei(I0_density, I2_temperature, a.density_np, a.Zeta);
+    const double scale = (-1.0) * lnee * a.kpre * a.Dt;
+    if (lane == 0) s.sc[0] = scale;
+    for (int k = lane; k < n; k += 32) {
+        double i2 = I2[k] * (4.0 * M_PI);
+        i2 /= vr[k] * vr[k];
+        const double i0 = I0[k] * (4.0 * M_PI);
+        const double j1m = J1m[k] * (4.0 * M_PI * vr[k]);
+        const double t1 = i0 + (2.0 * j1m - i2) / 3.0;
+        const double t2 = (i2 + j1m) / 3.0;
+        double sc = (k == 0) ? 0.0 : t1 * lnee;
+        sc += zlnei * I0_density;
+        sc /= pow(vr[k], 3);
+        sc *= a.kpre * a.Dt;
+        s.scat[k] = sc;
+        double ta = 0.0, tb = 0.0, tc = 0.0;
+        if (k == 0) {
+            tb = 8.0 * M_PI * f[0] * scale;
+        } else if (k < n - 1) {
+            const double IvDnDm1 = 1.0 / (vr[k] * 0.5 * (vr[k + 1] - vr[k - 1]) * (vr[k] - vr[k - 1]));
+            const double IvDnDp1 = 1.0 / (vr[k] * 0.5 * (vr[k + 1] - vr[k - 1]) * (vr[k + 1] - vr[k]));
+            const double Ivsq2Dn = 1.0 / (vr[k] * vr[k] * (vr[k + 1] - vr[k - 1]));
+            tb = (8.0 * M_PI * f[k] - t2 * (IvDnDm1 + IvDnDp1)) * scale;
+            ta = (t2 * IvDnDm1 - t1 * Ivsq2Dn) * scale;
+            tc = (t2 * IvDnDp1 + t1 * Ivsq2Dn) * scale;
+        }
+        s.tri_a[k] = ta; s.tri_b[k] = tb; s.tri_c[k] = tc;
+        // raw -df/dv at n-1/2 (finished below); f0 is free once the e-e step is done
+        s.f0[k] = (k >= 1) ? (f[k - 1] - f[k]) / (vr[k] - vr[k - 1]) : 0.0;
+    }
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+        double df, ddf;
+        if (k == 0) {
+            const double f00 = (f[0] - (vr[0] * vr[0] / (vr[1] * vr[1])) * f[1]) / (1.0 - (vr[0] * vr[0]) / (vr[1] * vr[1]));
+            ddf = 2.0 * (f[1] - f00) / (vr[1] * vr[1]);
+            df = ddf * vr[0];
+        } else if (k < n - 1) {
+            df = (f[k + 1] - f[k - 1]) / (vr[k + 1] - vr[k - 1]);
+            ddf = (s.f0[k] - s.f0[k + 1]) / (0.5 * (vr[k + 1] - vr[k - 1]));
+        } else {
+            df = 0.0;
+            ddf = s.f0[k];
+        }
+        if (k < n - 1) { df /= vr[k] * vr[k]; ddf /= 2.0 * vr[k]; }
+        s.df0[k] = df;
+        s.ddf0[k] = ddf;
+    }
+    __syncwarp();
+}
+
+template <typename TP>
+__device__ void tridiagonal_chunks(const CollideArgs& a, const Smem& s, long long cell) {
+    TP* planes = reinterpret_cast<TP*>(a.planes);
+    const int* plane_l = a.plane_l;
+    const int* plane_m = a.plane_m;
+    const int nplanes = a.nplanes;
+    const int n = a.np, ld = n + 1;
+    for (int q0 = 0; q0 < nplanes; q0 += a.chunk) {
+        const int nq = min(a.chunk, nplanes - q0);
+        // stage: d column of plane j at chunk[j*2*ld], c' column at chunk[j*2*ld + ld]
+        for (int idx = threadIdx.x; idx < nq * n; idx += blockDim.x) {
+            const int j = idx / n, p = idx - j * n;
+            s.chunk[(long long)j * 2 * ld + p] = (double)planes[(long long)(q0 + j) * a.pstride + cell * n + p];
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < nq; j += blockDim.x) {
+            const int q = q0 + j;
+            const int l = plane_l[q], m = plane_m[q];
+            if (l < 1 || m > a.mmax_coll || (l == 1 ? !a.do_l1 : !a.do_lm)) continue;
+            double* d = s.chunk + (long long)j * 2 * ld;
+            double* c = d + ld;
+            const double ll1 = l * ((-0.5) * (l + 1.0));
+            // Thomas, TridiagonalSolve (def-Nmethods.cpp:150-166)
+            double b0 = (l > 1 ? 0.0 : s.tri_b[0]) + (1.0 - ll1 * s.scat[0]);
+            c[0] = s.tri_c[0] / b0;
+            d[0] /= b0;
+            for (int i = 1; i < n; ++i) {
+                const double bi = s.tri_b[i] + (1.0 - ll1 * s.scat[i]);
+                const double id = 1.0 / (bi - c[i - 1] * s.tri_a[i]);
+                c[i] = s.tri_c[i] * id;
+                d[i] = (d[i] - d[i - 1] * s.tri_a[i]) * id;
+            }
+            for (int i = n - 2; i > -1; --i) d[i] = d[i] - c[i] * d[i + 1];
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < nq * n; idx += blockDim.x) {
+            const int j = idx / n, p = idx - j * n;
+            const int q = q0 + j;
+            const int l = plane_l[q], m = plane_m[q];
+            if (l < 1 || m > a.mmax_coll || (l == 1 ? !a.do_l1 : !a.do_lm)) continue;
+            planes[(long long)q * a.pstride + cell * n + p] = (TP)s.chunk[(long long)j * 2 * ld + p];
+        }
+        __syncthreads();
+    }
+}
+
+// dense path: assemble Alpha for harmonic order el in the CTA workspace
+__device__ void dense_assemble(const CollideArgs& a, const Smem& s, double* A, int el) {
+    const int n = a.np;
+    const double* vr = a.vr;
+    const double LL = el;
+    const double A1 = (LL + 1.0) * (LL + 2.0) / ((2.0 * LL + 1.0) * (2.0 * LL + 3.0));
+    const double A2 = (-1.0) * (LL - 1.0) * LL / ((2.0 * LL + 1.0) * (2.0 * LL - 1.0));
+    const double B1 = (-1.0) * (0.5 * LL * (LL + 1.0) + (LL + 1.0)) / ((2.0 * LL + 1.0) * (2.0 * LL + 3.0));
+    const double B2 = ((-0.5) * LL * (LL + 1.0) + (LL + 2.0)) / ((2.0 * LL + 1.0) * (2.0 * LL + 3.0));
+    const double B3 = (0.5 * LL * (LL + 1.0) + (LL - 1.0)) / ((2.0 * LL + 1.0) * (2.0 * LL - 1.0));
+    const double B4 = (0.5 * LL * (LL + 1.0) - LL) / ((2.0 * LL + 1.0) * (2.0 * LL - 1.0));
+    const double ll1 = el * ((-0.5) * (el + 1.0));
+    const double sc = s.sc[0];  // (-1) lnee kpre Dt (def-FokkerPlanck.cpp:973)
+    for (long long idx = threadIdx.x; idx < (long long)n * n; idx += blockDim.x) {
+        const int i = (int)(idx / n), j = (int)(idx - (long long)i * n);
+        double v = 0.0;
+        if (i == j) v = s.tri_b[i];
+        else if (j == i - 1) v = s.tri_a[i];
+        else if (j == i + 1) v = s.tri_c[i];
+        if (i == 0 && j == 0 && el > 1) v = 0.0;
+        if (i < n - 1 && j < n - 1) {
+            double t1 = A1 * s.ddf0[i] + B1 * s.df0[i]; t1 *= sc;
+            double t2 = A1 * s.ddf0[i] + B2 * s.df0[i]; t2 *= sc;
+            double t3 = A2 * s.ddf0[i] + B3 * s.df0[i]; t3 *= sc;
+            double t4 = A2 * s.ddf0[i] + B4 * s.df0[i]; t4 *= sc;
+            // same accumulation order as the reference row loop (def-FokkerPlanck.cpp:981-998)
+            if (j == 0) {
+                v += t1 * (2.0 * M_PI * pow(vr[0] / vr[i], el + 2) * vr[0] * vr[0] * (vr[1] - vr[0]));
+                v += t3 * (2.0 * M_PI * pow(vr[0] / vr[i], el) * vr[0] * vr[0] * (vr[1] - vr[0]));
+            }
+            if (j >= 1 && j < i) {
+                v += t1 * (2.0 * M_PI * pow(vr[j] / vr[i], el + 2) * vr[j] * vr[j] * (vr[j + 1] - vr[j - 1]));
+                v += t3 * (2.0 * M_PI * pow(vr[j] / vr[i], el) * vr[j] * vr[j] * (vr[j + 1] - vr[j - 1]));
+            }
+            if (j == i) {
+                // the reference reads vr[-1] at i = 0 (def-FokkerPlanck.cpp:989-990), a
+                // denormal malloc header word; 0 here
+                const double vlow = i > 0 ? vr[i - 1] : 0.0;
+                v += t1 * (2.0 * M_PI * vr[i] * vr[i] * (vr[i] - vlow));
+                v += t3 * (2.0 * M_PI * vr[i] * vr[i] * (vr[i] - vlow));
+                v += t2 * (2.0 * M_PI * vr[i] * vr[i] * (vr[i + 1] - vr[i]));
+                v += t4 * (2.0 * M_PI * vr[i] * vr[i] * (vr[i + 1] - vr[i]));
+            }
+            if (j > i) {
+                v += t2 * (2.0 * M_PI * pow(vr[j] / vr[i], -el - 1) * vr[j] * vr[j] * (vr[j + 1] - vr[j - 1]));
+                v += t4 * (2.0 * M_PI * pow(vr[j] / vr[i], -el + 1) * vr[j] * vr[j] * (vr[j + 1] - vr[j - 1]));
+            }
+        }
+        if (i == j) v += 1.0 - ll1 * s.scat[i];
+        A[idx] = v;
+    }
+}
+
+// Gauss_Seidel on one warp; x: complex (re at xr, im at xi) in smem, initial
+// guess = b.  Returns false (x untouched) when the dominance test fails.
+__device__ void dense_gauss_seidel(const double* A, int n, const double* inv, double* xr, double* xi,
+                                   const double* br, const double* bi, double* ovr, double* ovi) {
+    const int lane = threadIdx.x & 31;
+    const double tol = 1.0e-1;
+    int iteration = 0, conv = 0;
+    while ((iteration++ < 5) && (conv < n)) {
+        for (int k = lane; k < n; k += 32) { ovr[k] = xr[k]; ovi[k] = xi[k]; }
+        __syncwarp();
+        for (int i = 0; i < n; ++i) {
+            const double* row = A + (long long)i * n;
+            double sr = 0.0, si = 0.0;
+            for (int j = lane; j < n; j += 32) {
+                if (j == i) continue;
+                const double aij = row[j];
+                sr += aij * xr[j];
+                si += aij * xi[j];
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                sr += __shfl_xor_sync(kFull, sr, off);
+                si += __shfl_xor_sync(kFull, si, off);
+            }
+            if (lane == 0) {
+                xr[i] = inv[i] * (br[i] - sr);
+                xi[i] = inv[i] * (bi[i] - si);
+            }
+            __syncwarp();
+        }
+        // prefix convergence test |dx_i| < tol |x_i + 20 DBL_MIN|
+        conv = n;
+        for (int base = 0; base < n; base += 32) {
+            const int k = base + lane;
+            bool ok = true;
+            if (k < n) {
+                const double dr = ovr[k] - xr[k], di = ovi[k] - xi[k];
+                ok = hypot(dr, di) < tol * hypot(xr[k] + 20.0 * DBL_MIN, xi[k]);
+            }
+            const unsigned bad = __ballot_sync(kFull, !ok);
+            if (bad) { conv = base + __ffs(bad) - 1; break; }
+        }
+        __syncwarp();
+    }
+}
+
+template <typename TP>
+__device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell, double* A, double* scratch) {
+    TP* planes = reinterpret_cast<TP*>(a.planes);
+    const int* plane_of = a.plane_of;
+    const int n = a.np;
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    // per warp: x re/im, b re/im, old re/im (6n); shared: inv diag (n), dominance flag
+    double* inv = scratch;
+    int* dominant = reinterpret_cast<int*>(scratch + n);
+    double* wbase = scratch + n + 2 + warp * 6 * n;
+    double *xr = wbase, *xi = wbase + n, *br = wbase + 2 * n, *bi = wbase + 3 * n, *ovr = wbase + 4 * n,
+           *ovi = wbase + 5 * n;
+    for (int el = 1; el <= a.l0; ++el) {
+        if (el == 1 ? !a.do_l1 : !a.do_lm) continue;
+        dense_assemble(a, s, A, el);
+        __syncthreads();
+        if (threadIdx.x == 0) *dominant = 1;
+        __syncthreads();
+        // dominance: sequential signed row sums as in the reference
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double row = 0.0;
+            for (int j = 0; j < n; ++j) row += A[(long long)i * n + j];
+            if (!(row < 2.0 * A[(long long)i * n + i])) atomicExch(dominant, 0);
+            inv[i] = 1.0 / A[(long long)i * n + i];
+        }
+        __syncthreads();
+        const int mtop = min(el, a.mmax_coll);
+        if (*dominant) {
+            for (int m = warp; m <= mtop; m += nwarps) {
+                const long long q = plane_of[el * (a.m0 + 1) + m];
+                const TP* pr_ = planes + q * a.pstride + cell * n;
+                const TP* pi_ = planes + (q + 1) * a.pstride + cell * n;
+                for (int k = threadIdx.x & 31; k < n; k += 32) {
+                    br[k] = (double)pr_[k];
+                    bi[k] = m > 0 ? (double)pi_[k] : 0.0;
+                    xr[k] = br[k];
+                    xi[k] = bi[k];
+                }
+                __syncwarp();
+                dense_gauss_seidel(A, n, inv, xr, xi, br, bi, ovr, ovi);
+                TP* wr = planes + q * a.pstride + cell * n;
+                TP* wi = planes + (q + 1) * a.pstride + cell * n;
+                for (int k = threadIdx.x & 31; k < n; k += 32) {
+                    wr[k] = (TP)xr[k];
+                    if (m > 0) wi[k] = (TP)xi[k];
+                }
+                __syncwarp();
+            }
+        } else if (threadIdx.x == 0) {
+            atomicOr(a.status, 1);
+            atomicAdd(a.status + 1, mtop + 1);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideArgs a) {
+    extern __shared__ double smem[];
+    const int n = a.np;
+    Smem s = carve(smem, n);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) {
+        // f00 of the cell
+        for (int k = threadIdx.x; k < n; k += blockDim.x) s.f[k] = a.f00[cell * n + k];
+        __syncthreads();
+        if (warp == 0 && a.do_ee) {
+            for (int sub = 0; sub < a.nsub; ++sub) {
+                const double h = a.hsub;
+                for (int k = lane; k < n; k += 32) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
+                __syncwarp();
+                ee_slope(a, s, s.f1, s.fh);
+                for (int k = lane; k < n; k += 32) {
+                    double t = s.fh[k] * (0.5 * h);
+                    s.f1[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
+                }
+                __syncwarp();
+                ee_slope(a, s, s.f1, s.fh);
+                for (int k = lane; k < n; k += 32) {
+                    s.f1[k] = s.f0[k];
+                    double t = s.fh[k] * (0.5 * h);
+                    s.f1[k] += t; t *= 2.0 / 3.0; s.f[k] += t;
+                }
+                __syncwarp();
+                ee_slope(a, s, s.f1, s.fh);
+                for (int k = lane; k < n; k += 32) {
+                    double t = s.fh[k] * h;
+                    s.f0[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
+                }
+                __syncwarp();
+                ee_slope(a, s, s.f0, s.fh);
+                for (int k = lane; k < n; k += 32) s.f[k] += s.fh[k] * (h / 6.0);
+                __syncwarp();
+            }
+            for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
+        }
+        if (a.do_l1 || a.do_lm) {
+            if (warp == 0) flm_reset(a, s, s.f);
+            __syncthreads();
+            if (a.if_tridiagonal) {
+                if (a.planes_fp32) tridiagonal_chunks<float>(a, s, cell);
+                else tridiagonal_chunks<double>(a, s, cell);
+            } else {
+                double* A = a.dense_ws + (long long)blockIdx.x * n * n;
+                if (a.planes_fp32) dense_solves<float>(a, s, cell, A, s.chunk);
+                else dense_solves<double>(a, s, cell, A, s.chunk);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal) {
+    size_t base = ((size_t)kSmemArrays * np + kSmemScalars) * sizeof(double);
+    size_t extra;
+    if (if_tridiagonal) extra = (size_t)chunk * 2 * (np + 1) * sizeof(double);
+    else extra = ((size_t)np + 2 + (size_t)(kCollideThreads / 32) * 6 * np) * sizeof(double);
+    return base + extra;
+}
+
+int collide_max_chunk(int np, size_t smem_budget) {
+    size_t base = ((size_t)kSmemArrays * np + kSmemScalars) * sizeof(double);
+    if (smem_budget <= base) return 0;
+    size_t per = (size_t)2 * (np + 1) * sizeof(double);
+    return (int)((smem_budget - base) / per);
+}
+
+int collide_threads() { return kCollideThreads; }
+
+cudaError_t launch_collide(const CollideArgs& a, cudaStream_t st, size_t smem, int blocks) {
+    static bool attr_set = false;
+    static size_t attr_bytes = 0;
+    if (!attr_set || smem > attr_bytes) {
+        cudaError_t e = cudaFuncSetAttribute(collide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+        attr_bytes = smem;
+    }
+    collide_kernel<<<blocks, kCollideThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace oshun

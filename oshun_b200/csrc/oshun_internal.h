@@ -1,0 +1,97 @@
+// Internal declarations shared by the CUDA translation units of liboshun_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "oshun_b200.h"
+
+namespace oshun {
+
+// Largest m0 the RK-stage kernel is compiled for; each instantiation keeps
+// 3 x (MC+1) complex accumulators per thread.
+constexpr int kMaxM0 = 8;
+// Largest nump (threads of one cell row are one CTA dimension).
+constexpr int kMaxNp = 1024;
+
+// Coupling coefficients of one source harmonic (l,m).  Each names the target
+// it feeds; a coefficient of a target that does not exist is 0 and the
+// target slot is never stored.
+struct CoefLM {
+    double ex_g, ex_h;      // Ex*G -> (l+1,m),   Ex*H -> (l-1,m)
+    double em_g, em_h;      // Em*G -> (l+1,m+1), Em*H -> (l-1,m+1)   Em = Ey - i Ez
+    double ep_h, ep_g;      // Ep*H -> (l-1,m-1), Ep*G -> (l+1,m-1)   Ep = Ey + i Ez (Re if m = 1)
+    double ax_p, ax_m;      // x advection -> (l+1,m), (l-1,m)
+    double ay_pp, ay_mp;    // y advection -> (l+1,m+1), (l-1,m+1)
+    double ay_mm, ay_pm;    // y advection -> (l-1,m-1), (l+1,m-1)   (Re if m = 1)
+    double b_m;             // (Bz - i By) f -> (l,m-1)               (Re if m = 1)
+    double gfac;            // G = Dp f * gfac + H,  gfac = -(2l+1)/l
+    double invpax;          // H = f * invpax/p + Dp f, invpax = -2(l+1) dp
+    double hp0;             // H at the p0 cell = f(p1) * hp0
+};
+
+// Arguments of one fused RHS + RK4 stage launch.  TS is the storage and
+// arithmetic type of the l >= 1 planes and the fields; f00 is always FP64.
+template <typename TS>
+struct StageArgs {
+    const double* f00_in; const TS* pl_in; const TS* fld_in;   // stage input (F is evaluated here)
+    const double* f00_B;  const TS* pl_B;  const TS* fld_B;    // step base Y0
+    double* f00_A;        TS* pl_A;        TS* fld_A;          // RK accumulator Y
+    double* f00_out;      TS* pl_out;      TS* fld_out;        // next stage input (or the slope)
+    const CoefLM* coef;   // [(l0+1)*(m0+1)]
+    const int* plane_of;  // [(l0+1)*(m0+1)]: plane of Re f_lm (l >= 1), -1 otherwise
+    const double* inv_pr; // 1/p
+    const double* vr;     // p/gamma
+    const double* wj;     // current quadrature weight (4 pi/3 included)
+    long long cells;      // numx*numy
+    long long pstride;    // cells*nump (elements per plane)
+    int np, nx, ny, l0, m0;
+    int mode;             // 0: RK stage; 1: write the slope to *_out
+    int first;            // stage 1: A = B + t*c2 instead of A += t*c2
+    double c1, c2;        // t = k*c1; out = B + t; A (+)= t*c2
+    double g00_s, g00_inv, g00_gr;   // p0 extrapolation of f00 for G00
+    double idx, idy;      // -1/(2dx), -1/(2dy)
+};
+
+struct CollideArgs {
+    double* f00;          // FP64 f00 plane (in/out)
+    void* planes;         // l >= 1 planes (double or float)
+    int planes_fp32;
+    const int* plane_of;  // [(l0+1)*(m0+1)]
+    const int* plane_l;   // [nplanes]: l of each plane
+    const int* plane_m;   // [nplanes]: m of each plane
+    int nplanes;
+    long long cells, pstride;
+    int np, l0, m0, mmax_coll;   // harmonics m <= min(l, mmax_coll) are collided
+    int do_ee, do_l1, do_lm;
+    int if_tridiagonal;
+    int nsub;             // e-e RK4 substeps
+    double hsub;          // e-e substep
+    double Dt;            // implicit step
+    int NB;
+    double density_np, Zeta;
+    double c_kpre, kpre;  // 4pi/3 re kp, re kp
+    // velocity grid tables [np]
+    const double *vr, *U4, *U4m1, *U2, *U2m1, *U1, *U1m1, *U3, *Qn, *Pn;
+    int chunk;            // planes staged per pass (tridiagonal path)
+    double* dense_ws;     // dense path: np*np doubles per block
+    int* status;          // [0] flags, [1] non-dominant count
+};
+
+// launchers (return cudaError_t)
+cudaError_t launch_stage_fp64(const StageArgs<double>& a, int mc, cudaStream_t s);
+cudaError_t launch_stage_fp32(const StageArgs<float>& a, int mc, cudaStream_t s);
+cudaError_t launch_collide(const CollideArgs& a, cudaStream_t s, size_t smem_bytes, int blocks);
+size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal);
+int collide_max_chunk(int np, size_t smem_budget);
+int collide_threads();
+cudaError_t launch_nan_check(const double* f00, const void* planes, int planes_fp32, long long n_f00,
+                             long long n_planes, const void* fields, long long n_fields, int* status,
+                             cudaStream_t s);
+
+void set_error(const std::string& msg);
+
+}  // namespace oshun

@@ -1,0 +1,326 @@
+// Fused RHS + RK4-stage kernel: Actions::Adv (OSHUN-1/def-Actions.cpp:73-94)
+// evaluated on one stage input and folded straight into the stage update of
+// Runge_Kutta_4::advance_p1 (OSHUN-1/def-RK.cpp:110-145).
+//
+// Work decomposition.  One thread owns one (cell, p) point of every harmonic.
+// A CTA holds `blockDim.y` consecutive cells (x-major) and up to 256 momentum
+// cells of each; wider momentum rows are swept in chunks.  Each thread walks
+// the source harmonics row by row (l = 0..l0, all m of a row unrolled) and
+// scatters every coupling of source (l,m) into register accumulators of the
+// only target rows it can reach, l-1, l and l+1.  After source row l has
+// passed, target row l-1 has received all of its terms; it is RK-updated and
+// written at once, so the slope never touches HBM.  Per stage and plane HBM
+// sees one read of the stage input (p and x/y neighbours come from the same
+// lines through L1/L2), the reads of Y0 and Y and the writes of the next
+// stage input and Y: 3/5/5/3 words over the four stages.
+//
+// Couplings, per source (l,m), G/H as in MakeGH/G00
+// (OSHUN-1/def-VlasovMax.cpp:496-535), Dp = f[p-1]-f[p+1] with the reference's
+// ends (OSHUN-1/def-State.cpp:359-380):
+//   E field (Exyz, def-VlasovMax.cpp:346-491):
+//     Ex G -> (l+1,m), Ex H -> (l-1,m), Em G -> (l+1,m+1), Em H -> (l-1,m+1),
+//     Ep H -> (l-1,m-1), Ep G -> (l+1,m-1) (real part only when m = 1)
+//   B field (Bxyz, def-VlasovMax.cpp:597-644):
+//     (Bz+iBy)/2 f -> (l,m+1), -i m Bx f -> (l,m), (Bz-iBy) f -> (l,m-1)
+//   advection (Axy, def-VlasovMax.cpp:834-951), v = p/gamma:
+//     x: -> (l+1,m), (l-1,m);  y: -> (l+1,m+1), (l-1,m+1), (l-1,m-1), (l+1,m-1)
+//   current (Jxyz, def-VlasovMax.cpp:680-745): FP64 quadrature of f10, f11
+//   Ampere/Faraday (def-VlasovMax.cpp:979-1035) on the cell's neighbours
+//   CLEAN_LOW_PC (def-Actions.cpp:240-253): slope of l >= 2 zeroed for
+//   p < min(l-1, 80)
+#include "oshun_internal.h"
+
+namespace oshun {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxCellsPerCta = 8;
+constexpr int kPChunk = 256;
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+// out/B/A are base pointers (out may be null: stage 4 has no next input)
+template <typename TS>
+__device__ __forceinline__ void rk_update(const StageArgs<TS>& a, TS* out, const TS* B, TS* A,
+                                          long long i, TS k) {
+    if (a.mode == 1) { out[i] = k; return; }
+    const TS t = k * (TS)a.c1;
+    const TS b = B[i];
+    if (out) out[i] = b + t;
+    A[i] = (a.first ? b : A[i]) + t * (TS)a.c2;
+}
+
+__device__ __forceinline__ void rk_update_f00(double* out, const double* B, double* A, int mode,
+                                              int first, double c1, double c2, long long i, double k) {
+    if (mode == 1) { out[i] = k; return; }
+    const double t = k * c1;
+    const double b = B[i];
+    if (out) out[i] = b + t;
+    A[i] = (first ? b : A[i]) + t * c2;
+}
+
+template <int MC, typename TS>
+__global__ void __launch_bounds__(256) rk_stage_kernel(const StageArgs<TS> a) {
+    __shared__ double sj[3][kMaxCellsPerCta][kPChunk / 32];
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long cell = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+    const bool cv = cell < a.cells;
+    const int np = a.np;
+    const int mstride = a.m0 + 1;
+
+    long long cx = 0, cyy = 0;
+    if (cv) { cx = cell % a.nx; cyy = cell / a.nx; }
+    const long long cxm = cyy * a.nx + (cx == 0 ? a.nx - 1 : cx - 1);
+    const long long cxp = cyy * a.nx + (cx == a.nx - 1 ? 0 : cx + 1);
+    const long long cym = (cyy == 0 ? a.ny - 1 : cyy - 1) * (long long)a.nx + cx;
+    const long long cyp = (cyy == a.ny - 1 ? 0 : cyy + 1) * (long long)a.nx + cx;
+    const bool has_y = a.ny > 1;
+
+    TS ex = 0, ey = 0, ez = 0, bx = 0, by = 0, bz = 0;
+    if (cv) {
+        ex = ld(a.fld_in + cell);
+        ey = ld(a.fld_in + a.cells + cell);
+        ez = ld(a.fld_in + 2 * a.cells + cell);
+        bx = ld(a.fld_in + 3 * a.cells + cell);
+        by = ld(a.fld_in + 4 * a.cells + cell);
+        bz = ld(a.fld_in + 5 * a.cells + cell);
+    }
+
+    double jx = 0.0, jyr = 0.0, jyi = 0.0;
+
+    for (int pbase = 0; pbase < np; pbase += blockDim.x) {
+        const int p = pbase + threadIdx.x;
+        const bool pv = cv && p < np;
+        const long long o = cell * np + p;
+        const long long oxm = cxm * np + p, oxp = cxp * np + p;
+        const long long oym = cym * np + p, oyp = cyp * np + p;
+        const TS invp = pv ? (TS)ld(a.inv_pr + p) : TS(0);
+        const TS vr = pv ? (TS)ld(a.vr + p) : TS(0);
+        const double wj = pv ? ld(a.wj + p) : 0.0;
+
+        TS ar[3][MC + 1], ai[3][MC + 1];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) { ar[r][m] = 0; ai[r][m] = 0; }
+
+        // writes target row t (accumulators R, I) through the RK epilogue
+        auto epilogue = [&](int t, TS (&R)[MC + 1], TS (&I)[MC + 1]) {
+            const int nzero = t >= 2 ? min(t - 1, 80) : 0;
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) {
+                if (m > a.m0 || m > t) continue;
+                TS kr = R[m], ki = I[m];
+                if (p < nzero) { kr = 0; ki = 0; }
+                if (!pv) continue;
+                if (t == 0) {
+                    rk_update_f00(a.f00_out, a.f00_B, a.f00_A, a.mode, a.first, a.c1, a.c2, o, (double)kr);
+                } else {
+                    const long long q = ld(a.plane_of + t * mstride + m);
+                    rk_update(a, a.pl_out, a.pl_B, a.pl_A, q * a.pstride + o, kr);
+                    if (m > 0) rk_update(a, a.pl_out, a.pl_B, a.pl_A, (q + 1) * a.pstride + o, ki);
+                }
+            }
+        };
+
+        for (int s = 0; s <= a.l0; ++s) {
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) {
+                if (m > a.m0 || m > s) continue;
+                const CoefLM* c = a.coef + s * mstride + m;
+                const TS* src = nullptr;
+                if (s > 0) src = a.pl_in + (long long)ld(a.plane_of + s * mstride + m) * a.pstride;
+                auto load = [&](long long off, int comp) -> TS {
+                    if (s == 0) return (TS)ld(a.f00_in + off);
+                    return ld(src + comp * a.pstride + off);
+                };
+                // centre value and its p neighbours (shuffles; warp edges load)
+                TS fr = pv ? load(o, 0) : TS(0);
+                TS fi = (m > 0 && pv) ? load(o, 1) : TS(0);
+                TS frm = __shfl_up_sync(kFull, fr, 1), frp = __shfl_down_sync(kFull, fr, 1);
+                TS fim = TS(0), fip = TS(0);
+                if (m > 0) { fim = __shfl_up_sync(kFull, fi, 1); fip = __shfl_down_sync(kFull, fi, 1); }
+                if (pv && lane == 0 && p > 0) {
+                    frm = load(o - 1, 0);
+                    if (m > 0) fim = load(o - 1, 1);
+                }
+                if (pv && lane == 31 && p + 1 < np) {
+                    frp = load(o + 1, 0);
+                    if (m > 0) fip = load(o + 1, 1);
+                }
+                // G and H
+                TS Gr, Gi, Hr, Hi;
+                const TS dr = (p == 0) ? TS(0) : (p == np - 1 ? frm - fr : frm - frp);
+                const TS di = (p == 0) ? TS(0) : (p == np - 1 ? fim - fi : fim - fip);
+                if (s == 0) {
+                    Gr = dr; Gi = 0; Hr = 0; Hi = 0;
+                    if (p == 0) {
+                        const TS f00x = (fr - frp * (TS)a.g00_s) * (TS)a.g00_inv;
+                        Gr = (frp - f00x) * (TS)a.g00_gr;
+                    }
+                } else {
+                    const TS ipx = invp * (TS)ld(&c->invpax);
+                    const TS gf = (TS)ld(&c->gfac);
+                    Hr = fr * ipx + dr; Hi = fi * ipx + di;
+                    Gr = dr * gf + Hr;  Gi = di * gf + Hi;
+                    if (p == 0) {
+                        const TS hp0 = (TS)ld(&c->hp0);
+                        Gr = 0; Gi = 0; Hr = frp * hp0; Hi = fip * hp0;
+                    }
+                }
+                const int mp = m + 1 <= MC ? m + 1 : MC;
+                const int mm = m >= 1 ? m - 1 : 0;
+                // E field
+                {
+                    const TS cg = (TS)ld(&c->ex_g) * ex, ch = (TS)ld(&c->ex_h) * ex;
+                    ar[2][m] += cg * Gr; ai[2][m] += cg * Gi;
+                    ar[0][m] += ch * Hr; ai[0][m] += ch * Hi;
+                    if (m + 1 <= MC) {
+                        const TS eg = (TS)ld(&c->em_g), eh = (TS)ld(&c->em_h);
+                        ar[2][mp] += eg * (ey * Gr + ez * Gi); ai[2][mp] += eg * (ey * Gi - ez * Gr);
+                        ar[0][mp] += eh * (ey * Hr + ez * Hi); ai[0][mp] += eh * (ey * Hi - ez * Hr);
+                    }
+                    if (m >= 1) {
+                        const TS ph = (TS)ld(&c->ep_h), pg = (TS)ld(&c->ep_g);
+                        ar[0][mm] += ph * (ey * Hr - ez * Hi);
+                        ar[2][mm] += pg * (ey * Gr - ez * Gi);
+                        if (m >= 2) {
+                            ai[0][mm] += ph * (ey * Hi + ez * Hr);
+                            ai[2][mm] += pg * (ey * Gi + ez * Gr);
+                        }
+                    }
+                }
+                // B field
+                {
+                    if (m + 1 <= MC) {
+                        ar[1][mp] += TS(0.5) * (bz * fr - by * fi);
+                        ai[1][mp] += TS(0.5) * (bz * fi + by * fr);
+                    }
+                    if (m >= 1) {
+                        const TS mb = (TS)m * bx;
+                        ar[1][m] += mb * fi; ai[1][m] += -(mb * fr);
+                        const TS cb = (TS)ld(&c->b_m);
+                        ar[1][mm] += cb * (bz * fr + by * fi);
+                        if (m >= 2) ai[1][mm] += cb * (bz * fi - by * fr);
+                    }
+                }
+                // x advection
+                {
+                    const TS dxr = pv ? (load(oxm, 0) - load(oxp, 0)) * vr : TS(0);
+                    const TS dxi = (m > 0 && pv) ? (load(oxm, 1) - load(oxp, 1)) * vr : TS(0);
+                    const TS xp = (TS)ld(&c->ax_p), xm = (TS)ld(&c->ax_m);
+                    ar[2][m] += xp * dxr; ai[2][m] += xp * dxi;
+                    ar[0][m] += xm * dxr; ai[0][m] += xm * dxi;
+                }
+                // y advection
+                if (has_y) {
+                    const TS dyr = pv ? (load(oym, 0) - load(oyp, 0)) * vr : TS(0);
+                    const TS dyi = (m > 0 && pv) ? (load(oym, 1) - load(oyp, 1)) * vr : TS(0);
+                    if (m + 1 <= MC) {
+                        const TS pp = (TS)ld(&c->ay_pp), mp_ = (TS)ld(&c->ay_mp);
+                        ar[2][mp] += pp * dyr; ai[2][mp] += pp * dyi;
+                        ar[0][mp] += mp_ * dyr; ai[0][mp] += mp_ * dyi;
+                    }
+                    if (m >= 1) {
+                        const TS ym_ = (TS)ld(&c->ay_mm), yp_ = (TS)ld(&c->ay_pm);
+                        ar[0][mm] += ym_ * dyr; ar[2][mm] += yp_ * dyr;
+                        if (m >= 2) { ai[0][mm] += ym_ * dyi; ai[2][mm] += yp_ * dyi; }
+                    }
+                }
+                // current of f10 / f11, FP64 quadrature
+                if (s == 1) {
+                    if (m == 0) jx += wj * (double)fr;
+                    else if (m == 1) { jyr += wj * (double)fr; jyi += wj * (double)fi; }
+                }
+            }
+            if (s >= 1) epilogue(s - 1, ar[0], ai[0]);
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) {
+                ar[0][m] = ar[1][m]; ai[0][m] = ai[1][m];
+                ar[1][m] = ar[2][m]; ai[1][m] = ai[2][m];
+                ar[2][m] = 0;        ai[2][m] = 0;
+            }
+        }
+        epilogue(a.l0, ar[0], ai[0]);
+    }
+
+    // per-cell current: warp sums, then warps in order (deterministic)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        jx += __shfl_xor_sync(kFull, jx, off);
+        jyr += __shfl_xor_sync(kFull, jyr, off);
+        jyi += __shfl_xor_sync(kFull, jyi, off);
+    }
+    if (lane == 0) {
+        sj[0][threadIdx.y][warp] = jx;
+        sj[1][threadIdx.y][warp] = jyr;
+        sj[2][threadIdx.y][warp] = jyi;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0 || !cv) return;
+    double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
+    const int nw = (min(np, (int)blockDim.x) + 31) >> 5;
+    for (int w = 0; w < nw; ++w) { Jx += sj[0][threadIdx.y][w]; Jyr += sj[1][threadIdx.y][w]; Jyi += sj[2][threadIdx.y][w]; }
+
+    const TS* F = a.fld_in;
+    const long long C = a.cells;
+    const TS idx = (TS)a.idx, idy = (TS)a.idy;
+    // J: Ex += Jx, Ey += Re J11, Ez += -Im J11 with J11 = 2 * (f11 quadrature)
+    TS dEx = (TS)Jx;
+    TS dEy = (TS)(2.0 * Jyr);
+    TS dEz = (TS)(-(2.0 * Jyi));
+    dEx += idy * (ld(F + 5 * C + cym) - ld(F + 5 * C + cyp));
+    dEy += -idx * (ld(F + 5 * C + cxm) - ld(F + 5 * C + cxp));
+    dEz += -idy * (ld(F + 3 * C + cym) - ld(F + 3 * C + cyp));
+    dEz += idx * (ld(F + 4 * C + cxm) - ld(F + 4 * C + cxp));
+    TS dBx = -idy * (ld(F + 2 * C + cym) - ld(F + 2 * C + cyp));
+    TS dBy = idx * (ld(F + 2 * C + cxm) - ld(F + 2 * C + cxp));
+    TS dBz = idy * (ld(F + 0 * C + cym) - ld(F + 0 * C + cyp));
+    dBz += -idx * (ld(F + 1 * C + cxm) - ld(F + 1 * C + cxp));
+    rk_update(a, a.fld_out, a.fld_B, a.fld_A, 0 * C + cell, dEx);
+    rk_update(a, a.fld_out, a.fld_B, a.fld_A, 1 * C + cell, dEy);
+    rk_update(a, a.fld_out, a.fld_B, a.fld_A, 2 * C + cell, dEz);
+    rk_update(a, a.fld_out, a.fld_B, a.fld_A, 3 * C + cell, dBx);
+    rk_update(a, a.fld_out, a.fld_B, a.fld_A, 4 * C + cell, dBy);
+    rk_update(a, a.fld_out, a.fld_B, a.fld_A, 5 * C + cell, dBz);
+}
+
+template <typename TS, int MC>
+cudaError_t launch_mc(const StageArgs<TS>& a, cudaStream_t s) {
+    const int np_pad = ((a.np + 31) / 32) * 32;
+    const int tx = np_pad < kPChunk ? np_pad : kPChunk;
+    int cpb = kPChunk / tx;
+    if (cpb > kMaxCellsPerCta) cpb = kMaxCellsPerCta;
+    if (cpb < 1) cpb = 1;
+    const long long blocks = (a.cells + cpb - 1) / cpb;
+    rk_stage_kernel<MC, TS><<<dim3((unsigned)blocks), dim3(tx, cpb), 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename TS>
+cudaError_t launch_stage(const StageArgs<TS>& a, int mc, cudaStream_t s) {
+    switch (mc) {
+        case 0: return launch_mc<TS, 0>(a, s);
+        case 1: return launch_mc<TS, 1>(a, s);
+        case 2: return launch_mc<TS, 2>(a, s);
+        case 3: return launch_mc<TS, 3>(a, s);
+        case 4: return launch_mc<TS, 4>(a, s);
+        case 6: return launch_mc<TS, 6>(a, s);
+        case 8: return launch_mc<TS, 8>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_stage_fp64(const StageArgs<double>& a, int mc, cudaStream_t s) {
+    return launch_stage<double>(a, mc, s);
+}
+cudaError_t launch_stage_fp32(const StageArgs<float>& a, int mc, cudaStream_t s) {
+    return launch_stage<float>(a, mc, s);
+}
+
+}  // namespace oshun

@@ -1,0 +1,141 @@
+"""Synthetic, seeded workloads of the benchmark configurations.
+
+Every builder returns ``(cfg, f, fields, meta)``: ``cfg`` the oshun_cfg
+fields, ``f`` complex128 [Nh][numy][numx][nump] and ``fields`` complex128
+[6][numy][numx] in the reference's storage order (ind(l,m),
+OSHUN-1/def-State.cpp:420-427), ``meta`` a description.  Units are the
+reference's: p in m_e c, x in c/w_p, t in 1/w_p (OSHUN-1/def-Input.cpp:77-80).
+The Maxwellian is the reference's Gaussian_p normalisation,
+exp(-p^2/2pt^2)/((2 pi)^{3/2} pt^3) (OSHUN-1/def-Setup.cpp:500-533).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+WORKLOADS = ("weibel2d", "landau1d", "relax1d", "landau1d_large")
+
+
+def num_harmonics(l0: int, m0: int) -> int:
+    return ((m0 + 1) * (2 * l0 - m0 + 2)) // 2
+
+
+def ind(l: int, m: int, m0: int) -> int:
+    return (l * (l + 1)) // 2 + m if l < m0 + 1 else l * (m0 + 1) - (m0 * (m0 + 1)) // 2 + m
+
+
+def p_axis(nump: int, pmin: float, pmax: float) -> np.ndarray:
+    return np.arange(nump, dtype=np.float64) * ((pmax - pmin) / (nump - 1)) + pmin
+
+
+def maxwellian(p, pt):
+    return np.exp(-(p * p) / (2.0 * pt * pt)) / (np.sqrt(2.0 * np.pi) * 2.0 * np.pi * pt ** 3)
+
+
+def _base_cfg(**kw) -> dict:
+    cfg = dict(t0=0.0, NB_algorithms=4, if_tridiagonal=1, if_implicit1D=1, density_np=1e21, Zeta=1.0,
+               ymin=0.0, ymax=1.0, precision=0, flags=0, small_dt=1.0)
+    cfg.update(kw)
+    return cfg
+
+
+def weibel2d(precision: int = 0, seed: int = 7, nx: int = 128, ny: int = 128):
+    """2D2V Weibel-type: nx = ny = 128 periodic, lmax = mmax = 6, np = 96 to
+    p_max = 8 v_th, bi-Maxwellian T_x/T_y = 4 projected onto l = 0, 2 (m = 0)
+    with seeded m = 2 noise, seeded B_z noise of amplitude 1e-6, full E and B
+    update, anisotropic collisions (tridiagonal, the production setting of the
+    reference's paper decks) at nu/w_p ~ 1e-3, RK4 dt = 0.02/w_p."""
+    vth = 0.05
+    l0 = m0 = 6
+    nump = 96
+    pmax = 8.0 * vth
+    pmin = pmax / (2.0 * nump)
+    L = 2.0 * np.pi / 0.5            # k_min = 0.5 w_p/c
+    cfg = _base_cfg(l0=l0, m0=m0, nump=nump, numx=nx, numy=ny, pmin=pmin, pmax=pmax,
+                    xmin=0.0, xmax=L * (nx - 1) / nx, ymin=0.0, ymax=L * (ny - 1) / ny,
+                    dt=0.02, small_dt=0.05, if_implicit1D=0, if_tridiagonal=1,
+                    density_np=1e21, precision=precision)
+    rng = np.random.default_rng(seed)
+    p = p_axis(nump, pmin, pmax)
+    # bi-Maxwellian, anisotropy axis x (the polar axis of the harmonics)
+    Tx, Ty = (2.0 * vth) ** 2, vth ** 2
+    mu, w = np.polynomial.legendre.leggauss(64)
+    P, MU = np.meshgrid(p, mu, indexing="ij")
+    fb = np.exp(-(P * MU) ** 2 / (2 * Tx) - P ** 2 * (1 - MU ** 2) / (2 * Ty))
+    fb /= (2 * np.pi) ** 1.5 * np.sqrt(Tx) * Ty
+    f00 = 0.5 * (fb * w).sum(axis=1)
+    P2 = 0.5 * (3 * mu ** 2 - 1)
+    f20 = 2.5 * (fb * (w * P2)).sum(axis=1)
+    nh = num_harmonics(l0, m0)
+    f = np.zeros((nh, ny, nx, nump), np.complex128)
+    f[ind(0, 0, m0)] = f00[None, None, :]
+    f[ind(2, 0, m0)] = f20[None, None, :]
+    noise = 1e-6 * rng.standard_normal((ny, nx)) + 1e-6j * rng.standard_normal((ny, nx))
+    f[ind(2, 2, m0)] = noise[..., None] * f20[None, None, :]
+    fields = np.zeros((6, ny, nx), np.complex128)
+    fields[5] = 1e-6 * rng.standard_normal((ny, nx))
+    meta = dict(workload="weibel2d", nx=nx, ny=ny, lmax=l0, mmax=m0, np=nump, vth=vth,
+                anisotropy="Tx/Ty=4", collisions="ee + implicit flm, tridiagonal", dt=0.02)
+    return cfg, f, fields, meta
+
+
+def landau1d(precision: int = 0, nx: int = 64, nump: int = 64, l0: int = 8, alpha: float = 1e-3,
+             klam: float = 0.3, vth: float = 0.05):
+    """1D1P Landau damping: nx periodic cells over L = 2 pi/k with
+    k lambda_D = klam, v_th = 0.05c, np cells to 8 v_th, n = 1 + alpha cos kx,
+    E_x from Gauss's law, fixed neutralising ions, RK4 dt = 0.05/w_p."""
+    k = klam / vth
+    L = 2.0 * np.pi / k
+    pmax = 8.0 * vth
+    pmin = pmax / (2.0 * nump)
+    cfg = _base_cfg(l0=l0, m0=0, nump=nump, numx=nx, numy=1, pmin=pmin, pmax=pmax, xmin=0.0,
+                    xmax=L * (nx - 1) / nx, dt=0.05, precision=precision)
+    p = p_axis(nump, pmin, pmax)
+    x = np.arange(nx) * (L / nx)
+    n = 1.0 + alpha * np.cos(k * x)
+    f = np.zeros((num_harmonics(l0, 0), 1, nx, nump), np.complex128)
+    f[0, 0] = n[:, None] * maxwellian(p[None, :], vth)
+    fields = np.zeros((6, 1, nx), np.complex128)
+    fields[0, 0] = -alpha / k * np.sin(k * x)
+    meta = dict(workload="landau1d", nx=nx, np=nump, lmax=l0, klambdaD=klam, vth=vth, dt=0.05)
+    return cfg, f, fields, meta
+
+
+def landau1d_large(precision: int = 0):
+    """Landau damping at nx = 8192, np = 256, lmax = 16: 35.7 M coefficients."""
+    cfg, f, fields, meta = landau1d(precision, nx=8192, nump=256, l0=16)
+    meta["workload"] = "landau1d_large"
+    return cfg, f, fields, meta
+
+
+def relax1d(precision: int = 0, klam_ei: float = 0.1, nx: int = 256, nump: int = 128, vth: float = 0.05):
+    """Collisional relaxation with heat flow: nx = 256 periodic, T(x) = T0
+    (1 + 1e-3 sin kx), uniform density, Z = 1, lmax = 1, np = 128 to 10 v_th,
+    implicit f1 solve and the f00 e-e step every RK4 step."""
+    pmax = 10.0 * vth
+    pmin = pmax / (2.0 * nump)
+    density = 1e22
+    # electron-ion collision frequency at v_th from the reference's scattering
+    # term: nu ~ Z lnL_ei * re * kp / v_th^3 (def-FokkerPlanck.cpp:785-787, 872-879)
+    re = 2.8179402894e-13
+    kp = np.sqrt(4.0 * np.pi * density * re)
+    nu = 8.0 * re * kp / vth ** 3
+    lam_ei = vth / nu
+    k = klam_ei / lam_ei
+    L = 2.0 * np.pi / k
+    cfg = _base_cfg(l0=1, m0=0, nump=nump, numx=nx, numy=1, pmin=pmin, pmax=pmax, xmin=0.0,
+                    xmax=L * (nx - 1) / nx, dt=0.1 / nu, small_dt=0.1 / nu, density_np=density,
+                    precision=precision)
+    p = p_axis(nump, pmin, pmax)
+    x = np.arange(nx) * (L / nx)
+    T = vth * np.sqrt(1.0 + 1e-3 * np.sin(k * x))
+    f = np.zeros((2, 1, nx, nump), np.complex128)
+    f[0, 0] = maxwellian(p[None, :], T[:, None])
+    fields = np.zeros((6, 1, nx), np.complex128)
+    meta = dict(workload="relax1d", nx=nx, np=nump, lmax=1, klambda_ei=klam_ei, nu_ei=nu)
+    return cfg, f, fields, meta
+
+
+def build(name: str, precision: int = 0):
+    if name not in WORKLOADS:
+        raise KeyError(name)
+    return globals()[name](precision=precision)
