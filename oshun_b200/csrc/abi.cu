@@ -152,6 +152,7 @@ struct oshun_ctx {
     int* d_plane_l = nullptr;    // [nplanes]
     int* d_plane_m = nullptr;    // [nplanes]
     int* d_hplane = nullptr;     // [2*nh]: plane of Re (or -1 for f00), complex flag
+    int* d_seq = nullptr;        // [nh]: source harmonics in stream order, l | (m << 16)
     double* d_ptab = nullptr;    // inv_pr, vr, wj
     double* d_vtab = nullptr;    // vr, U4, U4m1, U2, U2m1, U1, U1m1, U3, Qn, Pn
     double* d_dense_ws = nullptr;
@@ -272,6 +273,7 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     a.mode = mode;
     a.g00_s = g00_s; a.g00_inv = g00_inv; a.g00_gr = g00_gr;
     a.idx = idx; a.idy = idy;
+    a.seq = d_seq; a.nh = nh; a.err = d_status;
     (void)out_set;
     return a;
 }
@@ -425,6 +427,11 @@ int build_tables(oshun_ctx* h) {
         CK(cudaMemcpy(h->d_plane_l, plane_l.data(), sizeof(int) * plane_l.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->d_plane_m, plane_m.data(), sizeof(int) * plane_m.size(), cudaMemcpyHostToDevice));
     }
+    std::vector<int> seq;
+    for (int l = 0; l <= l0; ++l)
+        for (int m = 0; m <= std::min(l, m0); ++m) seq.push_back(l | (m << 16));
+    CK(cudaMalloc(&h->d_seq, sizeof(int) * seq.size()));
+    CK(cudaMemcpy(h->d_seq, seq.data(), sizeof(int) * seq.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&h->d_hplane, sizeof(int) * hplane.size()));
     CK(cudaMemcpy(h->d_hplane, hplane.data(), sizeof(int) * hplane.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&h->d_ptab, sizeof(double) * ptab.size()));
@@ -516,7 +523,7 @@ void free_ctx(oshun_ctx* h) {
             if (h->graph[p][c]) cudaGraphExecDestroy(h->graph[p][c]);
     for (int i = 0; i < 4; ++i) { cudaFree(h->f00[i]); cudaFree(h->pl[i]); cudaFree(h->fld[i]); }
     cudaFree(h->d_coef); cudaFree(h->d_plane_of); cudaFree(h->d_plane_l); cudaFree(h->d_plane_m);
-    cudaFree(h->d_hplane); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
+    cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
     cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -54,6 +54,10 @@ struct StageArgs {
     double c1, c2;        // t = k*c1; out = B + t; A (+)= t*c2
     double g00_s, g00_inv, g00_gr;   // p0 extrapolation of f00 for G00
     double idx, idy;      // -1/(2dx), -1/(2dy)
+    // bulk-copy pipelined variant
+    const int* seq;       // [nh]: source harmonics in stream order, s | (m << 16)
+    int nh;
+    int* err;             // error word (bit 4: a pipeline wait timed out)
 };
 
 struct CollideArgs {
