@@ -171,6 +171,8 @@ struct oshun_ctx {
     int collide_chunk = 0;
     size_t collide_smem = 0;
     int collide_blocks = 0;
+    int tri_cpc = 0;       // cells per CTA of the tridiagonal collision kernel (0: staged-chunk kernel)
+    int tri_blocks = 0;
 
     // constants
     double dp = 0, idx = 0, idy = 0, g00_s = 0, g00_inv = 0, g00_gr = 0, c_kpre = 0, kpre = 0;
@@ -505,7 +507,11 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
 
 int enqueue_collide(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt) {
     CollideArgs a = collide_args(h, do_ee, do_l1, do_lm, nsub, hsub, Dt);
-    cudaError_t e = launch_collide(a, h->stream, h->collide_smem, h->collide_blocks);
+    cudaError_t e;
+    if (h->tri_cpc > 0)
+        e = launch_collide_tri(a, h->stream, h->tri_cpc, h->tri_blocks);
+    else
+        e = launch_collide(a, h->stream, h->collide_smem, h->collide_blocks);
     if (e != cudaSuccess) { set_error(std::string("collide launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
     return OSHUN_OK;
 }
@@ -598,6 +604,13 @@ int oshun_create(const oshun_cfg* cfg, oshun_handle* out) {
         h->collide_chunk = chunk;
         h->collide_smem = collide_smem_bytes(np, chunk, 1);
         h->collide_blocks = (int)std::min<long long>(h->cells, (long long)prop.multiProcessorCount * 16);
+        // one warp per cell: as many resident 1-warp CTAs as shared memory allows
+        const size_t per_cell = collide_tri_smem_per_cell(np, cfg->l0);
+        if (per_cell <= budget) {
+            h->tri_cpc = 1;
+            const long long per_sm = std::max<long long>(1, std::min<long long>(32, (long long)(228 * 1024) / (long long)per_cell));
+            h->tri_blocks = (int)std::min<long long>(h->cells, per_sm * prop.multiProcessorCount * 4);
+        }
     } else {
         h->collide_smem = collide_smem_bytes(np, 0, 0);
         if (h->collide_smem > budget) { set_error("nump too large for the dense collision path"); return fail(OSHUN_ERR_UNSUPPORTED); }

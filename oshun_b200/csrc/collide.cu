@@ -437,6 +437,39 @@ __device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell
     }
 }
 
+// e-e RK4 substeps of Explicit_EC_FP::loop on one warp (f00 of the cell in s.f)
+__device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
+    const int n = a.np;
+    const int lane = threadIdx.x & 31;
+    for (int sub = 0; sub < a.nsub; ++sub) {
+        const double h = a.hsub;
+        for (int k = lane; k < n; k += 32) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
+        __syncwarp();
+        ee_slope(a, s, s.f1, s.fh);
+        for (int k = lane; k < n; k += 32) {
+            double t = s.fh[k] * (0.5 * h);
+            s.f1[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
+        }
+        __syncwarp();
+        ee_slope(a, s, s.f1, s.fh);
+        for (int k = lane; k < n; k += 32) {
+            s.f1[k] = s.f0[k];
+            double t = s.fh[k] * (0.5 * h);
+            s.f1[k] += t; t *= 2.0 / 3.0; s.f[k] += t;
+        }
+        __syncwarp();
+        ee_slope(a, s, s.f1, s.fh);
+        for (int k = lane; k < n; k += 32) {
+            double t = s.fh[k] * h;
+            s.f0[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
+        }
+        __syncwarp();
+        ee_slope(a, s, s.f0, s.fh);
+        for (int k = lane; k < n; k += 32) s.f[k] += s.fh[k] * (h / 6.0);
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideArgs a) {
     extern __shared__ double smem[];
     const int n = a.np;
@@ -448,33 +481,7 @@ __global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideA
         for (int k = threadIdx.x; k < n; k += blockDim.x) s.f[k] = a.f00[cell * n + k];
         __syncthreads();
         if (warp == 0 && a.do_ee) {
-            for (int sub = 0; sub < a.nsub; ++sub) {
-                const double h = a.hsub;
-                for (int k = lane; k < n; k += 32) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
-                __syncwarp();
-                ee_slope(a, s, s.f1, s.fh);
-                for (int k = lane; k < n; k += 32) {
-                    double t = s.fh[k] * (0.5 * h);
-                    s.f1[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
-                }
-                __syncwarp();
-                ee_slope(a, s, s.f1, s.fh);
-                for (int k = lane; k < n; k += 32) {
-                    s.f1[k] = s.f0[k];
-                    double t = s.fh[k] * (0.5 * h);
-                    s.f1[k] += t; t *= 2.0 / 3.0; s.f[k] += t;
-                }
-                __syncwarp();
-                ee_slope(a, s, s.f1, s.fh);
-                for (int k = lane; k < n; k += 32) {
-                    double t = s.fh[k] * h;
-                    s.f0[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
-                }
-                __syncwarp();
-                ee_slope(a, s, s.f0, s.fh);
-                for (int k = lane; k < n; k += 32) s.f[k] += s.fh[k] * (h / 6.0);
-                __syncwarp();
-            }
+            ee_substeps(a, s);
             for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
         }
         if (a.do_l1 || a.do_lm) {
@@ -490,6 +497,127 @@ __global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideA
             }
         }
         __syncthreads();
+    }
+}
+
+__device__ __forceinline__ bool collided(const CollideArgs& a, int l, int m) {
+    return l >= 1 && m <= a.mmax_coll && (l == 1 ? a.do_l1 : a.do_lm);
+}
+
+// Tridiagonal collision step, one warp per cell (1-warp CTAs, one CTA per
+// cell), no CTA-wide barriers:
+//   1. f00 e-e substeps, reset_coeff, and the Thomas pivots of every l --
+//      c'_i and 1/(b_i - c'_{i-1} a_i), with b_0 kept for the reference's
+//      d_0/b_0 -- one lane per l (TridiagonalSolve, def-Nmethods.cpp:152-159).
+//   2. every collided plane of the cell: the row is loaded coalesced into
+//      shared memory and both recurrences of TridiagonalSolve run with lanes
+//      over momentum.  Each lane owns a contiguous run of p; the value
+//      entering its run comes from a warp scan of the affine maps
+//      d'_i = (d_i - a_i d'_{i-1}) id_i (forward) and x_i = d'_i - c'_i x_{i+1}
+//      (backward); inside the run the lane applies the reference's recursion.
+template <typename TP>
+__global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
+    extern __shared__ double smem[];
+    const int n = a.np;
+    const int l0 = a.l0;
+    const int lane = threadIdx.x & 31;
+    TP* planes = reinterpret_cast<TP*>(a.planes);
+    const bool solve = a.do_l1 || a.do_lm;
+    Smem s = carve(smem, n);
+    double* cp = s.chunk;                    // [l0][n]
+    double* idv = cp + (size_t)l0 * n;       // [l0][n]
+    double* row = idv + (size_t)l0 * n;      // [n]
+    const int E = (n + 31) >> 5;
+    const int rb = min(lane * E, n), re = min(rb + E, n);
+
+    for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) {
+        for (int k = lane; k < n; k += 32) s.f[k] = a.f00[cell * n + k];
+        __syncwarp();
+        if (a.do_ee) {
+            ee_substeps(a, s);
+            for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
+        }
+        if (!solve) continue;
+        flm_reset(a, s, s.f);
+        for (int l = 1 + lane; l <= l0; l += 32) {
+            if (!(l == 1 ? a.do_l1 : a.do_lm)) continue;
+            const double ll1 = l * ((-0.5) * (l + 1.0));
+            double* cpl = cp + (size_t)(l - 1) * n;
+            double* idl = idv + (size_t)(l - 1) * n;
+            const double b0 = (l > 1 ? 0.0 : s.tri_b[0]) + (1.0 - ll1 * s.scat[0]);
+            double cprev = s.tri_c[0] / b0;
+            cpl[0] = cprev;
+            idl[0] = b0;
+            for (int i = 1; i < n; ++i) {
+                const double bi = s.tri_b[i] + (1.0 - ll1 * s.scat[i]);
+                const double id = 1.0 / (bi - cprev * s.tri_a[i]);
+                cprev = s.tri_c[i] * id;
+                cpl[i] = cprev;
+                idl[i] = id;
+            }
+        }
+        __syncwarp();
+        const double* tri_a = s.tri_a;
+        for (int q = 0; q < a.nplanes; ++q) {
+            const int l = a.plane_l[q], m = a.plane_m[q];
+            if (!collided(a, l, m)) continue;
+            const double* cpl = cp + (size_t)(l - 1) * n;
+            const double* idl = idv + (size_t)(l - 1) * n;
+            TP* g = planes + (long long)q * a.pstride + cell * n;
+            for (int k = lane; k < n; k += 32) row[k] = (double)g[k];
+            __syncwarp();
+            // forward: compose this lane's maps x -> A x + B over [rb, re)
+            double A = 1.0, B = 0.0;
+            for (int i = rb; i < re; ++i) {
+                double Ai, Bi;
+                if (i == 0) { Ai = 0.0; Bi = row[0] / idl[0]; }
+                else { Ai = -(tri_a[i] * idl[i]); Bi = row[i] * idl[i]; }
+                B = Ai * B + Bi;
+                A = Ai * A;
+            }
+            // inclusive scan of the maps over the lanes (earlier lanes first)
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const double Ap = __shfl_up_sync(kFull, A, off), Bp = __shfl_up_sync(kFull, B, off);
+                if (lane >= off) { B = A * Bp + B; A = A * Ap; }
+            }
+            double din = __shfl_up_sync(kFull, B, 1);   // d' just before this lane's run
+            if (rb < re) {
+                double d = din;
+                for (int i = rb; i < re; ++i) {
+                    if (i == 0) d = row[0] / idl[0];
+                    else d = (row[i] - d * tri_a[i]) * idl[i];
+                    row[i] = d;
+                }
+            }
+            __syncwarp();
+            // backward: x_i = d'_i - c'_i x_{i+1}, x_{n-1} = d'_{n-1}
+            A = 1.0; B = 0.0;
+            for (int i = re - 1; i >= rb; --i) {
+                double Ai, Bi;
+                if (i == n - 1) { Ai = 0.0; Bi = row[i]; }
+                else { Ai = -cpl[i]; Bi = row[i]; }
+                B = Ai * B + Bi;
+                A = Ai * A;
+            }
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const double Ap = __shfl_down_sync(kFull, A, off), Bp = __shfl_down_sync(kFull, B, off);
+                if (lane + off < 32) { B = A * Bp + B; A = A * Ap; }
+            }
+            double xin = __shfl_down_sync(kFull, B, 1);  // x just after this lane's run
+            if (rb < re) {
+                double x = xin;
+                for (int i = re - 1; i >= rb; --i) {
+                    if (i == n - 1) x = row[i];
+                    else x = row[i] - cpl[i] * x;
+                    row[i] = x;
+                }
+            }
+            __syncwarp();
+            for (int k = lane; k < n; k += 32) g[k] = (TP)row[k];
+            __syncwarp();
+        }
     }
 }
 
@@ -513,15 +641,40 @@ int collide_max_chunk(int np, size_t smem_budget) {
 int collide_threads() { return kCollideThreads; }
 
 cudaError_t launch_collide(const CollideArgs& a, cudaStream_t st, size_t smem, int blocks) {
-    static bool attr_set = false;
     static size_t attr_bytes = 0;
-    if (!attr_set || smem > attr_bytes) {
+    if (smem > attr_bytes) {
         cudaError_t e = cudaFuncSetAttribute(collide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
         attr_bytes = smem;
     }
     collide_kernel<<<blocks, kCollideThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+size_t collide_tri_smem_per_cell(int np, int l0) {
+    return ((size_t)kSmemArrays * np + kSmemScalars + 2 * (size_t)l0 * np + np) * sizeof(double);
+}
+
+cudaError_t launch_collide_tri(const CollideArgs& a, cudaStream_t st, int /*cells_per_cta*/, int blocks) {
+    const size_t smem = collide_tri_smem_per_cell(a.np, a.l0);
+    static size_t attr64 = 0, attr32 = 0;
+    if (a.planes_fp32) {
+        if (smem > attr32) {
+            cudaError_t e = cudaFuncSetAttribute(collide_warp_kernel<float>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr32 = smem;
+        }
+        collide_warp_kernel<float><<<blocks, 32, smem, st>>>(a);
+    } else {
+        if (smem > attr64) {
+            cudaError_t e = cudaFuncSetAttribute(collide_warp_kernel<double>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr64 = smem;
+        }
+        collide_warp_kernel<double><<<blocks, 32, smem, st>>>(a);
+    }
     return cudaGetLastError();
 }
 

@@ -19,8 +19,9 @@ constexpr int kMaxNp = 1024;
 
 // Coupling coefficients of one source harmonic (l,m).  Each names the target
 // it feeds; a coefficient of a target that does not exist is 0 and the
-// target slot is never stored.
-struct CoefLM {
+// target slot is never stored.  16-byte aligned, 128 bytes: the kernels copy
+// entries with 128-bit loads and stores.
+struct alignas(16) CoefLM {
     double ex_g, ex_h;      // Ex*G -> (l+1,m),   Ex*H -> (l-1,m)
     double em_g, em_h;      // Em*G -> (l+1,m+1), Em*H -> (l-1,m+1)   Em = Ey - i Ez
     double ep_h, ep_g;      // Ep*H -> (l-1,m-1), Ep*G -> (l+1,m-1)   Ep = Ey + i Ez (Re if m = 1)
@@ -32,6 +33,7 @@ struct CoefLM {
     double invpax;          // H = f * invpax/p + Dp f, invpax = -2(l+1) dp
     double hp0;             // H at the p0 cell = f(p1) * hp0
 };
+static_assert(sizeof(CoefLM) == 128 && alignof(CoefLM) == 16, "CoefLM layout");
 
 // Arguments of one fused RHS + RK4 stage launch.  TS is the storage and
 // arithmetic type of the l >= 1 planes and the fields; f00 is always FP64.
@@ -92,6 +94,8 @@ cudaError_t launch_collide(const CollideArgs& a, cudaStream_t s, size_t smem_byt
 size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal);
 int collide_max_chunk(int np, size_t smem_budget);
 int collide_threads();
+size_t collide_tri_smem_per_cell(int np, int l0);
+cudaError_t launch_collide_tri(const CollideArgs& a, cudaStream_t s, int cells_per_cta, int blocks);
 cudaError_t launch_nan_check(const double* f00, const void* planes, int planes_fp32, long long n_f00,
                              long long n_planes, const void* fields, long long n_fields, int* status,
                              cudaStream_t s);

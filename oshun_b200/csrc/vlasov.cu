@@ -49,7 +49,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxCellsPerCta = 8;
 constexpr int kPChunk = 256;
-constexpr int kDepth = 4;
+constexpr int kDepth = 6;
 constexpr long long kWaitLimit = 1ll << 22;   // mbarrier try_wait rounds before giving up
 
 template <typename T>
@@ -516,49 +516,78 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tma_kernel(const StageArgs<T
         if (need_B && lane == 0) mbar_arrive(rowempty + rb);
     };
 
+    // consume source harmonic `id` (already landed) of order (s, m)
+    auto consume = [&](const int s, const int m, const int id) {
+        const unsigned char* sb = slots + (size_t)(id % kDepth) * L.slot_bytes;
+        const int seg = L.seg_cells * np;
+        auto rd = [&](int comp, int cs, int pp) -> TS {
+            if constexpr (sizeof(TS) == 8) {
+                return reinterpret_cast<const TS*>(sb)[comp * seg + cs * np + pp];
+            } else {
+                if (s == 0) return (TS)reinterpret_cast<const double*>(sb)[cs * np + pp];
+                return reinterpret_cast<const TS*>(sb)[comp * seg + cs * np + pp];
+            }
+        };
+        TS fr = 0, fi = 0, frm = 0, frp = 0, fim = 0, fip = 0, dxr = 0, dxi = 0, dyr = 0, dyi = 0;
+        if (pv) {
+            fr = rd(0, 1 + c, p);
+            if (p > 0) frm = rd(0, 1 + c, p - 1);
+            if (p + 1 < np) frp = rd(0, 1 + c, p + 1);
+            dxr = (rd(0, c, p) - rd(0, c + 2, p)) * vr;
+            if (has_y) dyr = (rd(0, tx + 2 + c, p) - rd(0, 2 * tx + 2 + c, p)) * vr;
+            if (m > 0) {
+                fi = rd(1, 1 + c, p);
+                if (p > 0) fim = rd(1, 1 + c, p - 1);
+                if (p + 1 < np) fip = rd(1, 1 + c, p + 1);
+                dxi = (rd(1, c, p) - rd(1, c + 2, p)) * vr;
+                if (has_y) dyi = (rd(1, tx + 2 + c, p) - rd(1, 2 * tx + 2 + c, p)) * vr;
+            }
+        }
+        // 128-bit broadcast loads of the coupling table entry
+        CoefLM cc;
+        {
+            const double2* src2 = reinterpret_cast<const double2*>(scoef + s * mstride + m);
+            double2* dst2 = reinterpret_cast<double2*>(&cc);
+#pragma unroll
+            for (int k = 0; k < (int)(sizeof(CoefLM) / sizeof(double2)); ++k) dst2[k] = src2[k];
+        }
+        couple<MC, TS>(ar, ai, m, s, cc, fr, fi, frm, frp, fim, fip, dxr, dxi, dyr, dyi, has_y, p, np, invp, ex,
+                       ey, ez, bx, by, bz, a.g00_s, a.g00_inv, a.g00_gr);
+        if (s == 1) {
+            if (m == 0) jx += wj * (double)fr;
+            else if (m == 1) { jyr += wj * (double)fr; jyi += wj * (double)fi; }
+        }
+    };
+
+    // harmonics are consumed in pairs behind one wait, so the compiler can
+    // interleave the two instruction streams
     int idx = 0;
     for (int s = 0; s <= a.l0; ++s) {
+        const int mtop = min(s, a.m0);
 #pragma unroll
-        for (int m = 0; m <= MC; ++m) {
-            if (m > a.m0 || m > s) continue;
-            const int slot = idx % kDepth;
-            if (!dead && !mbar_wait(full + slot, (uint32_t)((idx / kDepth) & 1))) {
+        for (int mp = 0; mp <= MC; mp += 2) {
+            if (mp > mtop) continue;
+            const bool two = (mp + 1 <= MC) && (mp + 1 <= mtop);
+            if (!dead && !mbar_wait(full + (idx % kDepth), (uint32_t)((idx / kDepth) & 1))) {
+                atomicOr(a.err, 16);
+                dead = true;
+            }
+            if (two && !dead && !mbar_wait(full + ((idx + 1) % kDepth), (uint32_t)(((idx + 1) / kDepth) & 1))) {
                 atomicOr(a.err, 16);
                 dead = true;
             }
             if (!dead) {
-                const unsigned char* sb = slots + (size_t)slot * L.slot_bytes;
-                const int seg = L.seg_cells * np;
-                auto rd = [&](int comp, int cs, int pp) -> TS {
-                    if (s == 0) return (TS)reinterpret_cast<const double*>(sb)[cs * np + pp];
-                    return reinterpret_cast<const TS*>(sb)[comp * seg + cs * np + pp];
-                };
-                TS fr = 0, fi = 0, frm = 0, frp = 0, fim = 0, fip = 0, dxr = 0, dxi = 0, dyr = 0, dyi = 0;
-                if (pv) {
-                    fr = rd(0, 1 + c, p);
-                    if (p > 0) frm = rd(0, 1 + c, p - 1);
-                    if (p + 1 < np) frp = rd(0, 1 + c, p + 1);
-                    dxr = (rd(0, c, p) - rd(0, c + 2, p)) * vr;
-                    if (has_y) dyr = (rd(0, tx + 2 + c, p) - rd(0, 2 * tx + 2 + c, p)) * vr;
-                    if (m > 0) {
-                        fi = rd(1, 1 + c, p);
-                        if (p > 0) fim = rd(1, 1 + c, p - 1);
-                        if (p + 1 < np) fip = rd(1, 1 + c, p + 1);
-                        dxi = (rd(1, c, p) - rd(1, c + 2, p)) * vr;
-                        if (has_y) dyi = (rd(1, tx + 2 + c, p) - rd(1, 2 * tx + 2 + c, p)) * vr;
-                    }
-                }
-                const CoefLM cc = scoef[s * mstride + m];
-                couple<MC, TS>(ar, ai, m, s, cc, fr, fi, frm, frp, fim, fip, dxr, dxi, dyr, dyi, has_y, p, np,
-                               invp, ex, ey, ez, bx, by, bz, a.g00_s, a.g00_inv, a.g00_gr);
-                if (s == 1) {
-                    if (m == 0) jx += wj * (double)fr;
-                    else if (m == 1) { jyr += wj * (double)fr; jyi += wj * (double)fi; }
+                consume(s, mp, idx);
+                if (mp + 1 <= MC) {
+                    if (two) consume(s, mp + 1, idx + 1);
                 }
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(empty + slot);   // this warp is done with the slot
-            ++idx;
+            if (lane == 0) {                          // this warp is done with the slot(s)
+                mbar_arrive(empty + (idx % kDepth));
+                if (two) mbar_arrive(empty + ((idx + 1) % kDepth));
+            }
+            idx += two ? 2 : 1;
         }
         if (s >= 1) epilogue(s - 1);
         rotate_rows<MC, TS>(ar, ai);
