@@ -62,7 +62,23 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
         sys.stderr.write(r.stderr)
         raise RuntimeError("link failed")
     os.replace(tmp, LIB)
+    build_host(verbose)
     return LIB
+
+
+def build_host(verbose: bool = False) -> str:
+    """The C++ example driver over the host layer (host/oshun.hpp)."""
+    src = os.path.join(HERE, "host", "oshun_main_loop.cpp")
+    out = os.path.join(HERE, "host", "oshun_main_loop")
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-I", INCLUDE, "-I", os.path.join(HERE, "host"), src,
+           "-L", HERE, "-loshun_b200", "-Wl,-rpath,$ORIGIN/..", "-o", out]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stderr)
+        raise RuntimeError("host driver build failed")
+    return out
 
 
 if __name__ == "__main__":

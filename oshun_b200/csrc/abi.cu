@@ -154,7 +154,7 @@ struct oshun_ctx {
     int* d_hplane = nullptr;     // [2*nh]: plane of Re (or -1 for f00), complex flag
     int* d_seq = nullptr;        // [nh]: source harmonics in stream order, l | (m << 16)
     double* d_ptab = nullptr;    // inv_pr, vr, wj
-    double* d_vtab = nullptr;    // vr, U4, U4m1, U2, U2m1, U1, U1m1, U3, Qn, Pn
+    double* d_vtab = nullptr;    // vr, U4, U4m1, U2, U2m1, U1, U1m1, U3, Qn, Pn, v^5, v^7
     double* d_dense_ws = nullptr;
     int dense_blocks = 0;
     int* d_status = nullptr;
@@ -395,7 +395,7 @@ int build_tables(oshun_ctx* h) {
     h->nplanes = q;
 
     // velocity grid of the collision operators (def-FokkerPlanck.cpp:143-172, 790-803)
-    std::vector<double> vt((size_t)10 * np, 0.0);
+    std::vector<double> vt((size_t)12 * np, 0.0);
     double* V = vt.data();
     for (int i = 0; i < np; ++i) V[i] = vr[i];
     for (int i = 1; i < np; ++i) {
@@ -407,7 +407,11 @@ int build_tables(oshun_ctx* h) {
         V[5 * np + i] = 0.5 * vr[i] * dv;
         V[6 * np + i] = 0.5 * vr[i - 1] * dv;
     }
-    for (int i = 0; i < np; ++i) V[7 * np + i] = std::pow(vr[i], 3);
+    for (int i = 0; i < np; ++i) {
+        V[7 * np + i] = std::pow(vr[i], 3);
+        V[10 * np + i] = std::pow(vr[i], 5);
+        V[11 * np + i] = std::pow(vr[i], 7);
+    }
     V[8 * np + 0] = 1.0 / ((vr[0] * vr[0] * vr[1]) / 2.0);
     for (int i = 1; i < np - 1; ++i) V[8 * np + i] = 1.0 / (vr[i] * vr[i] * (vr[i + 1] - vr[i - 1]) / 2.0);
     for (int i = 0; i < np - 1; ++i) V[9 * np + i] = 1.0 / ((vr[i + 1] - vr[i]) / 2.0 * (vr[i + 1] + vr[i]));
@@ -499,6 +503,7 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     const double* V = h->d_vtab;
     a.vr = V; a.U4 = V + np; a.U4m1 = V + 2 * np; a.U2 = V + 3 * np; a.U2m1 = V + 4 * np;
     a.U1 = V + 5 * np; a.U1m1 = V + 6 * np; a.U3 = V + 7 * np; a.Qn = V + 8 * np; a.Pn = V + 9 * np;
+    a.V5 = V + 10 * np; a.V7 = V + 11 * np;
     a.chunk = h->collide_chunk;
     a.dense_ws = h->d_dense_ws;
     a.status = h->d_status;

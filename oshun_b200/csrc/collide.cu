@@ -139,9 +139,11 @@ __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin,
         double g;
         if (k < a.NB) {
             const double f00 = (fin[0] - fin[1] * v0s / v1s) / (1.0 - v0s / v1s);
-            const double i2s = f00 * pow(vr[k], 3) / 3.0 + (fin[1] - f00) * pow(vr[k], 5) / v1s * 0.2;
-            const double i4s = f00 * pow(vr[k], 5) * 0.2 + (fin[1] - f00) * pow(vr[k], 7) / (v1s * 7.0);
-            g = fin[k] * i4s + (pow(vr[k], 3) * fin[k] - 3.0 * i2s) * s.J1[k];
+            // v^3, v^5, v^7 tabulated on the host with the same pow() the reference calls
+            const double v3 = a.U3[k], v5 = a.V5[k], v7 = a.V7[k];
+            const double i2s = f00 * v3 / 3.0 + (fin[1] - f00) * v5 / v1s * 0.2;
+            const double i4s = f00 * v5 * 0.2 + (fin[1] - f00) * v7 / (v1s * 7.0);
+            g = fin[k] * i4s + (v3 * fin[k] - 3.0 * i2s) * s.J1[k];
         } else {
             double i2 = s.I2[k] * s.J1[k];
             i2 *= -3.0;
@@ -197,7 +199,7 @@ __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) 
         const double t2 = (i2 + j1m) / 3.0;
         double sc = (k == 0) ? 0.0 : t1 * lnee;
         sc += zlnei * I0_density;
-        sc /= pow(vr[k], 3);
+        sc /= a.U3[k];
         sc *= a.kpre * a.Dt;
         s.scat[k] = sc;
         double ta = 0.0, tb = 0.0, tc = 0.0;

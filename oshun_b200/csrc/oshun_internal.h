@@ -81,7 +81,7 @@ struct CollideArgs {
     double density_np, Zeta;
     double c_kpre, kpre;  // 4pi/3 re kp, re kp
     // velocity grid tables [np]
-    const double *vr, *U4, *U4m1, *U2, *U2m1, *U1, *U1m1, *U3, *Qn, *Pn;
+    const double *vr, *U4, *U4m1, *U2, *U2m1, *U1, *U1m1, *U3, *Qn, *Pn, *V5, *V7;
     int chunk;            // planes staged per pass (tridiagonal path)
     double* dense_ws;     // dense path: np*np doubles per block
     int* status;          // [0] flags, [1] non-dominant count

@@ -49,7 +49,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxCellsPerCta = 8;
 constexpr int kPChunk = 256;
-constexpr int kDepth = 6;
+constexpr int kDepth = 10;
 constexpr long long kWaitLimit = 1ll << 22;   // mbarrier try_wait rounds before giving up
 
 template <typename T>
