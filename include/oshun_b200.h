@@ -142,6 +142,33 @@ int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields,
 /* Plane index of the real part of harmonic (l,m) in `planes` (the imaginary
  * part, m > 0, follows it), or -1 for (0,0), which lives in `f00`. */
 int oshun_plane_index(oshun_handle h, int l, int m, int* plane);
+/* ---- allocation-free collision step --------------------------------------- */
+
+/* No counterpart in the reference.  The implicit f_lm collision step (the work
+ * of oshun_collide_f1 followed by oshun_collide_flm, over Dt) on device planes
+ * the caller owns, for callers that cannot allocate device memory in their
+ * time loop (an application that gives all device memory to its own pool at
+ * start-up, or a foreign runtime that owns every device buffer).  The call
+ * allocates nothing: its tables and, in the dense Gauss-Seidel mode, its
+ * matrix workspace live in a fixed 32 MiB __device__ array that every GPU
+ * loading the library holds until exit.
+ *   cfg        the run configuration; precision must be OSHUN_FP64; limits
+ *              l0 <= 64, m0 <= 8, nump <= 1024 and one nump x nump FP64
+ *              matrix within the 32 MiB (OSHUN_ERR_UNSUPPORTED beyond them)
+ *   f00        device pointer, FP64 f00 plane [numy][numx][nump] (read)
+ *   planes     device pointer, the l >= 1 planes in the layout of
+ *              oshun_device_state / oshun_plane_index, FP64 (read/written)
+ *   Dt         implicit step (Euler_Backward's t_new - t)
+ *   stream     cudaStream_t (NULL: the default stream)
+ *   nondominant  optional: when not NULL the call waits for the stream and
+ *              stores the number of Gauss-Seidel solves skipped as not
+ *              diagonally dominant
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Every call shares the array and it keeps the
+ * last call's contents: calls that overlap on the GPU race on it. */
+int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, double* planes, double Dt, void* stream,
+                              long long* nondominant);
+
 /* Human-readable message of the last error on this thread. */
 const char* oshun_last_error(void);
 int oshun_abi_version(void);

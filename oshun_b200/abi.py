@@ -25,7 +25,7 @@ EXPORTED = [
     "oshun_create", "oshun_destroy", "oshun_set_stream", "oshun_synchronize", "oshun_upload",
     "oshun_download", "oshun_rhs", "oshun_rk4_step", "oshun_collide_ee", "oshun_collide_f1",
     "oshun_collide_flm", "oshun_step", "oshun_time", "oshun_status_flags", "oshun_device_state",
-    "oshun_plane_index", "oshun_last_error", "oshun_abi_version",
+    "oshun_plane_index", "oshun_last_error", "oshun_abi_version", "oshun_collide_flm_noalloc",
 ]
 
 
@@ -79,6 +79,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
     lib.oshun_plane_index.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.oshun_collide_flm_noalloc.argtypes = [ctypes.POINTER(OshunCfg), vp, vp, ctypes.c_double, vp,
+                                              ctypes.POINTER(ctypes.c_longlong)]
     lib.oshun_last_error.restype = ctypes.c_char_p
     lib.oshun_abi_version.restype = ctypes.c_int
     _lib = lib
