@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liboshun_b200.so")
+# OSHUN_B200_LIB points at another build of the library (default: the in-tree one)
+LIB_PATH = os.environ.get("OSHUN_B200_LIB") or os.path.join(HERE, "liboshun_b200.so")
 
 OSHUN_FP64 = 0
 OSHUN_FP32_SPLIT = 1

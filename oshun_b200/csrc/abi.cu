@@ -609,12 +609,11 @@ int oshun_create(const oshun_cfg* cfg, oshun_handle* out) {
         h->collide_chunk = chunk;
         h->collide_smem = collide_smem_bytes(np, chunk, 1);
         h->collide_blocks = (int)std::min<long long>(h->cells, (long long)prop.multiProcessorCount * 16);
-        // one warp per cell: as many resident 1-warp CTAs as shared memory allows
+        // one warp per cell: one 1-warp CTA per cell (grid-stride beyond 2^30 cells)
         const size_t per_cell = collide_tri_smem_per_cell(np, cfg->l0);
         if (per_cell <= budget) {
             h->tri_cpc = 1;
-            const long long per_sm = std::max<long long>(1, std::min<long long>(32, (long long)(228 * 1024) / (long long)per_cell));
-            h->tri_blocks = (int)std::min<long long>(h->cells, per_sm * prop.multiProcessorCount * 4);
+            h->tri_blocks = (int)std::min<long long>(h->cells, 1ll << 30);
         }
     } else {
         h->collide_smem = collide_smem_bytes(np, 0, 0);

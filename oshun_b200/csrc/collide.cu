@@ -30,49 +30,43 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCollideThreads = 128;
 
-// forward cumulative sum: out[k] = sum_{i=1..k} term(i), out[0] = 0
-template <class F>
-__device__ void warp_cumsum_fwd(double* out, int n, F term) {
+// The three cumulative integrals of one f on one warp, interleaved:
+//   I4[k] = sum_{i=1..k} U4[i] f[i] + U4m1[i] f[i-1]
+//   I2[k] = sum_{i=1..k} U2[i] f[i] + U2m1[i] f[i-1]
+//   J1[k] = sum_{i=k+1..n-1} U1[i] f[i] + U1m1[i] f[i-1]
+// Each lane sums a contiguous run of k, the lanes' run totals are combined
+// by a warp scan, and the lane then accumulates its run again from the
+// scanned start; the three chains are independent and interleaved.
+template <class T4, class T2, class T1>
+__device__ void warp_cumsum3(double* I4, double* I2, double* J1, int n, T4 t4, T2 t2, T1 t1) {
     const int lane = threadIdx.x & 31;
     const int E = (n + 31) >> 5;
     const int b = min(lane * E, n), e = min(b + E, n);
-    double loc = 0.0;
+    double l4 = 0.0, l2 = 0.0, l1 = 0.0;
     for (int k = b; k < e; ++k)
-        if (k > 0) loc += term(k);
-    double incl = loc;
+        if (k > 0) { l4 += t4(k); l2 += t2(k); }
+    for (int i = b + 1; i <= e && i <= n - 1; ++i) l1 += t1(i);
+    double s4 = l4, s2 = l2, s1 = l1;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        const double v = __shfl_up_sync(kFull, incl, off);
-        if (lane >= off) incl += v;
+        const double v4 = __shfl_up_sync(kFull, s4, off);
+        const double v2 = __shfl_up_sync(kFull, s2, off);
+        const double v1 = __shfl_down_sync(kFull, s1, off);
+        if (lane >= off) { s4 += v4; s2 += v2; }
+        if (lane + off < 32) s1 += v1;
     }
-    double run = __shfl_up_sync(kFull, incl, 1);
-    if (lane == 0) run = 0.0;
+    double r4 = __shfl_up_sync(kFull, s4, 1), r2 = __shfl_up_sync(kFull, s2, 1);
+    double r1 = __shfl_down_sync(kFull, s1, 1);
+    if (lane == 0) { r4 = 0.0; r2 = 0.0; }
+    if (lane == 31) r1 = 0.0;
     for (int k = b; k < e; ++k) {
-        if (k > 0) run += term(k);
-        out[k] = run;
+        if (k > 0) { r4 += t4(k); r2 += t2(k); }
+        I4[k] = r4;
+        I2[k] = r2;
     }
-    __syncwarp();
-}
-
-// backward cumulative sum: out[k] = sum_{i=k+1..n-1} term(i), out[n-1] = 0
-template <class F>
-__device__ void warp_cumsum_bwd(double* out, int n, F term) {
-    const int lane = threadIdx.x & 31;
-    const int E = (n + 31) >> 5;
-    const int b = min(lane * E, n), e = min(b + E, n);
-    double loc = 0.0;
-    for (int i = b + 1; i <= e && i <= n - 1; ++i) loc += term(i);
-    double incl = loc;  // suffix sum over lanes >= lane
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const double v = __shfl_down_sync(kFull, incl, off);
-        if (lane + off < 32) incl += v;
-    }
-    double run = __shfl_down_sync(kFull, incl, 1);
-    if (lane == 31) run = 0.0;
     for (int k = e - 1; k >= b; --k) {
-        if (k + 1 <= n - 1) run += term(k + 1);
-        out[k] = run;
+        if (k + 1 <= n - 1) r1 += t1(k + 1);
+        J1[k] = r1;
     }
     __syncwarp();
 }
@@ -128,9 +122,9 @@ __device__ Smem carve(double* base, int np) {
 __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin, double* fh) {
     const int n = a.np;
     const int lane = threadIdx.x & 31;
-    warp_cumsum_fwd(s.I4, n, [&](int k) { return a.U4[k] * fin[k] + a.U4m1[k] * fin[k - 1]; });
-    warp_cumsum_fwd(s.I2, n, [&](int k) { return a.U2[k] * fin[k] + a.U2m1[k] * fin[k - 1]; });
-    warp_cumsum_bwd(s.J1, n, [&](int i) { return a.U1[i] * fin[i] + a.U1m1[i] * fin[i - 1]; });
+    warp_cumsum3(s.I4, s.I2, s.J1, n, [&](int k) { return a.U4[k] * fin[k] + a.U4m1[k] * fin[k - 1]; },
+                 [&](int k) { return a.U2[k] * fin[k] + a.U2m1[k] * fin[k - 1]; },
+                 [&](int i) { return a.U1[i] * fin[i] + a.U1m1[i] * fin[i - 1]; });
     const double lnee = log_ee(4.0 * M_PI * s.I2[n - 1], 4.0 * M_PI * s.I4[n - 1], a.density_np);
     const double* vr = a.vr;
     const double v0s = vr[0] * vr[0], v1s = vr[1] * vr[1];
@@ -181,9 +175,9 @@ __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) 
     double* I2 = s.I4;   // reuse the e-e work arrays
     double* I0 = s.I2;
     double* J1m = s.J1;
-    warp_cumsum_fwd(I2, n, [&](int k) { return a.U4[k] * f[k] + a.U4m1[k] * f[k - 1]; });
-    warp_cumsum_fwd(I0, n, [&](int k) { return a.U2[k] * f[k] + a.U2m1[k] * f[k - 1]; });
-    warp_cumsum_bwd(J1m, n, [&](int i) { return a.U1[i] * f[i] + a.U1m1[i] * f[i - 1]; });
+    warp_cumsum3(I2, I0, J1m, n, [&](int k) { return a.U4[k] * f[k] + a.U4m1[k] * f[k - 1]; },
+                 [&](int k) { return a.U2[k] * f[k] + a.U2m1[k] * f[k - 1]; },
+                 [&](int i) { return a.U1[i] * f[i] + a.U1m1[i] * f[i - 1]; });
     const double I2_temperature = I2[n - 1] * (4.0 * M_PI);
     const double I0_density = I0[n - 1] * (4.0 * M_PI);
     const double lnee = log_ee(I0_density, I2_temperature, a.density_np);
@@ -623,6 +617,223 @@ __global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
     }
 }
 
+// Tridiagonal collision step for nump <= 32 E, one warp per cell (1-warp
+// CTAs, grid-stride over cells), rows in registers:
+//   1. f00 e-e substeps and reset_coeff as above; then the Thomas pivots of
+//      every l, one lane per l: c'_i and 1/(b_i - c'_{i-1} a_i)
+//      (TridiagonalSolve, def-Nmethods.cpp:152-159), 1/b_0 at i = 0.
+//   2. the collided planes of one l in batches of P: lane j holds p in
+//      [jE, jE+E) of each row in registers (the next batch's rows are loaded
+//      while this one is solved).  Both recurrences of TridiagonalSolve --
+//      d'_i = (d_i - a_i d'_{i-1}) / (b_i - c'_{i-1} a_i) forward,
+//      x_i = d'_i - c'_i x_{i+1} backward -- are affine maps of the previous
+//      value.  Each lane composes its run, a warp scan gives the value entering
+//      the run, and the lane applies the recursion inside its run.  The maps'
+//      multipliers depend on l only, so their composition and scan are done
+//      once per l and only the offsets are scanned per plane.
+// Shared memory (doubles): 4 scalars, tri_a, tri_b, tri_c, scat, then the
+// e-e/reset work arrays, which the per-l pivots overwrite once reset_coeff
+// is done.
+__device__ Smem carve_lane(double* base, int np) {
+    Smem s;
+    s.sc = base;
+    s.tri_a = base + 4; s.tri_b = s.tri_a + np; s.tri_c = s.tri_b + np; s.scat = s.tri_c + np;
+    s.df0 = s.scat + np; s.ddf0 = s.df0 + np;
+    s.f = s.ddf0 + np; s.f0 = s.f + np; s.f1 = s.f0 + np; s.fh = s.f1 + np;
+    s.I4 = s.fh + np; s.I2 = s.I4 + np; s.J1 = s.I2 + np;
+    s.chunk = s.df0;   // pivots: [l-1][c' (np), 1/pivot (np)]
+    return s;
+}
+__host__ __device__ inline size_t lane_smem_doubles(int np, int l0) {
+    const size_t work = 9 * (size_t)np, piv = 2 * (size_t)l0 * np;
+    return 4 + 4 * (size_t)np + (work > piv ? work : piv);
+}
+
+template <typename TP, int E, int P>
+__global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
+    extern __shared__ double smem[];
+    const int n = a.np;
+    const int l0 = a.l0;
+    const int lane = threadIdx.x & 31;
+    TP* planes = reinterpret_cast<TP*>(a.planes);
+    const bool solve = a.do_l1 || a.do_lm;
+    const Smem s = carve_lane(smem, n);
+    double* piv = s.chunk;
+    const int i0 = lane * E;   // first p of this lane's run
+
+    // plane batches: l, first plane, count (planes of one l are consecutive)
+    auto batch_first = [&](int& l, int& j) {
+        l = 1; j = 0;
+        while (l <= l0 && !collided(a, l, 0)) ++l;
+    };
+    auto batch_next = [&](int& l, int& j) {
+        const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
+        j += P;
+        if (j < nq) return;
+        j = 0;
+        do { ++l; } while (l <= l0 && !collided(a, l, 0));
+    };
+    auto load_batch = [&](long long cell, int l, int j, double (&r)[P][E]) {
+        if (l > l0) return;
+        const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
+        const long long q0 = a.plane_of[l * (a.m0 + 1)] + j;
+#pragma unroll
+        for (int b = 0; b < P; ++b) {
+            const TP* g = planes + (q0 + b) * a.pstride + cell * n;
+#pragma unroll
+            for (int e = 0; e < E; ++e) r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] : 0.0;
+        }
+    };
+
+    double cur[P][E], nxt[P][E];
+    for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) {
+        int bl, bj;
+        batch_first(bl, bj);
+        if (solve) load_batch(cell, bl, bj, cur);   // in flight during the e-e step
+        for (int k = lane; k < n; k += 32) s.f[k] = a.f00[cell * n + k];
+        __syncwarp();
+        if (a.do_ee) {
+            ee_substeps(a, s);
+            for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
+        }
+        if (!solve) continue;
+        flm_reset(a, s, s.f);
+        // pivots of every collided l, one lane per l
+        for (int l = 1 + lane; l <= l0; l += 32) {
+            if (!collided(a, l, 0)) continue;
+            const double ll1 = l * ((-0.5) * (l + 1.0));
+            double* cpl = piv + (size_t)(l - 1) * 2 * n;
+            double* idl = cpl + n;
+            const double b0 = (l > 1 ? 0.0 : s.tri_b[0]) + (1.0 - ll1 * s.scat[0]);
+            double cprev = s.tri_c[0] / b0;
+            cpl[0] = cprev;
+            idl[0] = 1.0 / b0;
+            for (int i = 1; i < n; ++i) {
+                const double bi = s.tri_b[i] + (1.0 - ll1 * s.scat[i]);
+                const double id = 1.0 / (bi - cprev * s.tri_a[i]);
+                cprev = s.tri_c[i] * id;
+                cpl[i] = cprev;
+                idl[i] = id;
+            }
+        }
+        __syncwarp();
+        // this lane's tri_a (forward multiplier -a_i id_i)
+        double ta[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) ta[e] = (i0 + e < n) ? s.tri_a[i0 + e] : 0.0;
+
+        int cl = -1;   // l of the per-l constants below
+        double id[E], cp[E], Af[5], Ab[5];
+        while (bl <= l0) {
+            const int l = bl, j = bl <= l0 ? bj : 0;
+            const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
+            int nl = bl, nj = bj;
+            batch_next(nl, nj);
+            if (nl <= l0) load_batch(cell, nl, nj, nxt);
+            if (l != cl) {
+                // per-l constants: pivots of this lane's run and the scan multipliers
+                cl = l;
+                const double* cpl = piv + (size_t)(l - 1) * 2 * n;
+                const double* idl = cpl + n;
+                double A = 1.0, B = 1.0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int i = i0 + e;
+                    id[e] = i < n ? idl[i] : 0.0;
+                    cp[e] = i < n ? cpl[i] : 0.0;
+                    if (i < n) A = (i == 0) ? 0.0 : A * (-(ta[e] * id[e]));
+                }
+#pragma unroll
+                for (int e = E - 1; e >= 0; --e) {
+                    const int i = i0 + e;
+                    if (i < n) B = (i == n - 1) ? 0.0 : B * (-cp[e]);
+                }
+#pragma unroll
+                for (int k = 0, off = 1; k < 5; ++k, off <<= 1) {
+                    Af[k] = A;
+                    Ab[k] = B;
+                    const double Ap = __shfl_up_sync(kFull, A, off);
+                    const double Bp = __shfl_down_sync(kFull, B, off);
+                    if (lane >= off) A *= Ap;
+                    if (lane + off < 32) B *= Bp;
+                }
+            }
+            // forward: run offsets, scan, recursion inside the run
+            double Bf[P];
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                double B = 0.0;
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int i = i0 + e;
+                    if (i < n) B = (i == 0) ? cur[b][e] * id[e] : (cur[b][e] - B * ta[e]) * id[e];
+                }
+                Bf[b] = B;
+            }
+#pragma unroll
+            for (int k = 0, off = 1; k < 5; ++k, off <<= 1) {
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const double Bp = __shfl_up_sync(kFull, Bf[b], off);
+                    if (lane >= off) Bf[b] += Af[k] * Bp;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                double d = __shfl_up_sync(kFull, Bf[b], 1);
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int i = i0 + e;
+                    if (i < n) {
+                        d = (i == 0) ? cur[b][e] * id[e] : (cur[b][e] - d * ta[e]) * id[e];
+                        cur[b][e] = d;
+                    }
+                }
+            }
+            // backward
+            double Bb[P];
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                double B = 0.0;
+#pragma unroll
+                for (int e = E - 1; e >= 0; --e) {
+                    const int i = i0 + e;
+                    if (i < n) B = (i == n - 1) ? cur[b][e] : cur[b][e] - cp[e] * B;
+                }
+                Bb[b] = B;
+            }
+#pragma unroll
+            for (int k = 0, off = 1; k < 5; ++k, off <<= 1) {
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const double Bp = __shfl_down_sync(kFull, Bb[b], off);
+                    if (lane + off < 32) Bb[b] += Ab[k] * Bp;
+                }
+            }
+            const long long q0 = a.plane_of[l * (a.m0 + 1)] + j;
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                double x = __shfl_down_sync(kFull, Bb[b], 1);
+                TP* g = planes + (q0 + b) * a.pstride + cell * n;
+#pragma unroll
+                for (int e = E - 1; e >= 0; --e) {
+                    const int i = i0 + e;
+                    if (i < n) {
+                        x = (i == n - 1) ? cur[b][e] : cur[b][e] - cp[e] * x;
+                        if (j + b < nq) g[i] = (TP)x;
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < P; ++b)
+#pragma unroll
+                for (int e = 0; e < E; ++e) cur[b][e] = nxt[b][e];
+            bl = nl; bj = nj;
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
 size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal) {
@@ -654,11 +865,47 @@ cudaError_t launch_collide(const CollideArgs& a, cudaStream_t st, size_t smem, i
 }
 
 size_t collide_tri_smem_per_cell(int np, int l0) {
+    if (np <= 256) return lane_smem_doubles(np, l0) * sizeof(double);
     return ((size_t)kSmemArrays * np + kSmemScalars + 2 * (size_t)l0 * np + np) * sizeof(double);
 }
 
+namespace {
+template <typename TP, int E>
+cudaError_t launch_lane(const CollideArgs& a, cudaStream_t st, int blocks, size_t smem) {
+    // planes per batch: two row sets of P x E doubles stay in registers
+    constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
+    static size_t attr = 0;
+    if (smem > attr) {
+        cudaError_t e = cudaFuncSetAttribute(collide_lane_kernel<TP, E, P>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = smem;
+    }
+    collide_lane_kernel<TP, E, P><<<blocks, 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+template <typename TP>
+cudaError_t launch_lane_e(const CollideArgs& a, cudaStream_t st, int blocks, size_t smem) {
+    switch ((a.np + 31) / 32) {
+        case 1: return launch_lane<TP, 1>(a, st, blocks, smem);
+        case 2: return launch_lane<TP, 2>(a, st, blocks, smem);
+        case 3: return launch_lane<TP, 3>(a, st, blocks, smem);
+        case 4: return launch_lane<TP, 4>(a, st, blocks, smem);
+        case 5: return launch_lane<TP, 5>(a, st, blocks, smem);
+        case 6: return launch_lane<TP, 6>(a, st, blocks, smem);
+        case 7: return launch_lane<TP, 7>(a, st, blocks, smem);
+        case 8: return launch_lane<TP, 8>(a, st, blocks, smem);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
 cudaError_t launch_collide_tri(const CollideArgs& a, cudaStream_t st, int /*cells_per_cta*/, int blocks) {
     const size_t smem = collide_tri_smem_per_cell(a.np, a.l0);
+    if (a.np <= 256) {
+        if (a.planes_fp32) return launch_lane_e<float>(a, st, blocks, smem);
+        return launch_lane_e<double>(a, st, blocks, smem);
+    }
     static size_t attr64 = 0, attr32 = 0;
     if (a.planes_fp32) {
         if (smem > attr32) {

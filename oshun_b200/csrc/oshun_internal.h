@@ -88,6 +88,9 @@ struct CollideArgs {
 };
 
 // launchers (return cudaError_t)
+// pipelined stage kernel (stage_pipe.cu); cudaErrorNotSupported when the shape does not fit
+template <typename TS>
+cudaError_t launch_stage_pipe(const StageArgs<TS>& a, int mc, cudaStream_t s);
 cudaError_t launch_stage_fp64(const StageArgs<double>& a, int mc, cudaStream_t s);
 cudaError_t launch_stage_fp32(const StageArgs<float>& a, int mc, cudaStream_t s);
 cudaError_t launch_collide(const CollideArgs& a, cudaStream_t s, size_t smem_bytes, int blocks);
