@@ -115,10 +115,18 @@ def landau1d_large(precision: int = 0):
     return cfg, f, fields, meta
 
 
-def relax1d(precision: int = 0, klam_ei: float = 0.1, nx: int = 256, nump: int = 128, vth: float = 0.05):
+def relax1d(precision: int = 0, klam_ei: float = 0.1, nx: int = 256, nump: int = 128, vth: float = 0.05,
+            dt: float | None = None, ee_substeps: int = 10):
     """Collisional relaxation with heat flow: nx = 256 periodic, T(x) = T0
     (1 + 1e-3 sin kx), uniform density, Z = 1, lmax = 1, np = 128 to 10 v_th,
-    implicit f1 solve and the f00 e-e step every RK4 step."""
+    implicit f1 solve and the f00 e-e step every step.
+
+    dt defaults to 0.1/nu_ei.  The reference's f00 e-e step is explicit RK4
+    subcycled at small_dt (Explicit_EC_FP::loop, def-FokkerPlanck.cpp:590-625);
+    at dt = 0.1/nu_ei it needs ~10 substeps to stay stable, so small_dt =
+    dt/ee_substeps.  The explicit RK4 Vlasov-Maxwell step is stable only for
+    w_p dt and v dt/dx of order 1, far below 0.1/nu_ei: at that dt the
+    configuration runs collision steps only."""
     pmax = 10.0 * vth
     pmin = pmax / (2.0 * nump)
     density = 1e22
@@ -130,8 +138,10 @@ def relax1d(precision: int = 0, klam_ei: float = 0.1, nx: int = 256, nump: int =
     lam_ei = vth / nu
     k = klam_ei / lam_ei
     L = 2.0 * np.pi / k
+    if dt is None:
+        dt = 0.1 / nu
     cfg = _base_cfg(l0=1, m0=0, nump=nump, numx=nx, numy=1, pmin=pmin, pmax=pmax, xmin=0.0,
-                    xmax=L * (nx - 1) / nx, dt=0.1 / nu, small_dt=0.1 / nu, density_np=density,
+                    xmax=L * (nx - 1) / nx, dt=dt, small_dt=dt / ee_substeps, density_np=density,
                     precision=precision)
     p = p_axis(nump, pmin, pmax)
     x = np.arange(nx) * (L / nx)
@@ -141,6 +151,55 @@ def relax1d(precision: int = 0, klam_ei: float = 0.1, nx: int = 256, nump: int =
     fields = np.zeros((6, 1, nx), np.complex128)
     meta = dict(workload="relax1d", nx=nx, np=nump, lmax=1, klambda_ei=klam_ei, nu_ei=nu)
     return cfg, f, fields, meta
+
+
+def density_for_nu(nu: float, vth: float) -> float:
+    """Electron density (1/cm^3) whose collision frequency at v_th is nu (in
+    w_p): the inverse of relax1d's nu = 8 re kp / v_th^3, kp = sqrt(4 pi n re)."""
+    re = 2.8179402894e-13
+    kp = nu * vth ** 3 / (8.0 * re)
+    return kp * kp / (4.0 * np.pi * re)
+
+
+def batch_problems(n: int = 512, seed: int = 2024, precision: int = 1, vth: float = 0.05, klam: float = 0.3):
+    """Independent 1D problems of uneven size: nx in [32, 512], np in [32,
+    256] and lmax in [1, 16] drawn log-uniform from `seed` and rounded (np to
+    a multiple of 4, the bulk copies' 16-byte rule for FP32 rows), each a
+    Maxwellian with a density perturbation of amplitude 1e-3 and random phase
+    over L = 2 pi/k, k lambda_D = 0.3, np to 8 v_th, nu/w_p uniform in
+    [0, 1e-2] (one problem in eight collisionless, nu = 0), FP32 bulk.  dt =
+    min(0.05, 0.5 dx/v_max) keeps the explicit advection stable.
+    Returns [(cfg, f, fields, collide)], meta."""
+    rng = np.random.default_rng(seed)
+    k = klam / vth
+    L = 2.0 * np.pi / k
+    pmax = 8.0 * vth
+    vmax = pmax / np.sqrt(1 + pmax * pmax)
+    out = []
+    ncoef = 0
+    for i in range(n):
+        nx = int(round(np.exp(rng.uniform(np.log(32), np.log(512)))))
+        nump = int(round(np.exp(rng.uniform(np.log(32), np.log(256))) / 4.0)) * 4
+        l0 = int(round(np.exp(rng.uniform(np.log(1), np.log(16)))))
+        phase = rng.uniform(0, 2 * np.pi)
+        nu = 0.0 if i % 8 == 7 else rng.uniform(0.0, 1e-2)
+        dx = L / nx
+        dt = min(0.05, 0.5 * dx / vmax)
+        pmin = pmax / (2.0 * nump)
+        density = density_for_nu(nu, vth) if nu > 0 else 1e21
+        cfg = _base_cfg(l0=l0, m0=0, nump=nump, numx=nx, numy=1, pmin=pmin, pmax=pmax, xmin=0.0,
+                        xmax=L * (nx - 1) / nx, dt=dt, small_dt=dt, density_np=density, precision=precision)
+        p = p_axis(nump, pmin, pmax)
+        x = np.arange(nx) * dx
+        dens = 1.0 + 1e-3 * np.cos(k * x + phase)
+        f = np.zeros((num_harmonics(l0, 0), 1, nx, nump), np.complex128)
+        f[0, 0] = dens[:, None] * maxwellian(p[None, :], vth)
+        fields = np.zeros((6, 1, nx), np.complex128)
+        fields[0, 0] = -1e-3 / k * np.sin(k * x + phase)
+        out.append((cfg, f, fields, nu > 0))
+        ncoef += nx * nump * (l0 + 1)
+    meta = dict(workload=f"batch{n}", problems=n, seed=seed, coefficients=ncoef)
+    return out, meta
 
 
 def build(name: str, precision: int = 0):
