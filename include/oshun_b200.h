@@ -142,6 +142,41 @@ int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields,
 /* Plane index of the real part of harmonic (l,m) in `planes` (the imaginary
  * part, m > 0, follows it), or -1 for (0,0), which lives in `f00`. */
 int oshun_plane_index(oshun_handle h, int l, int m, int* plane);
+/* ---- batches of independent problems -------------------------------------- */
+
+/* No counterpart in the reference, whose runs are one problem per process
+ * (the loop over runs a caller would write around main_loop).  A batch holds
+ * n independent problems of one precision, any mix of l0, m0 <= 8, nump <=
+ * 256 (nump x element size a multiple of 16 bytes), numx, numy and dt, each
+ * with its own state and clocks.  oshun_batch_step advances every problem by
+ * one small step of its own dt per step (oshun_step's sequence) with one
+ * captured CUDA graph per step: four persistent stage launches over the
+ * (problem, tile) list of the whole batch and one collision launch per group
+ * of problems with equal ceil(nump/32).  collide[i] = 0 (or collide = NULL
+ * for all on) skips problem i's collision calls; collisional problems need
+ * if_tridiagonal = 1. */
+typedef struct oshun_batch_ctx* oshun_batch;
+int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_batch* out);
+int oshun_batch_destroy(oshun_batch b);
+int oshun_batch_size(oshun_batch b, int* n);
+/* the handle of problem i (owned by the batch; its queries and transfers work,
+ * its stream is the batch's) */
+int oshun_batch_problem(oshun_batch b, int i, oshun_handle* h);
+int oshun_batch_upload(oshun_batch b, int i, const double* harmonics, const double* fields);
+int oshun_batch_download(oshun_batch b, int i, double* harmonics, double* fields);
+int oshun_batch_step(oshun_batch b, int nsteps);
+/* OR of every problem's status word (oshun_status_flags) and bit 4 = a
+ * pipeline wait of a batched launch ran out. */
+int oshun_batch_status(oshun_batch b, int* flags);
+/* Stage tiles: consumer threads per CTA (32..256, a multiple of 32, at least
+ * the widest padded nump of the batch) and cells per tile at most (1..8). */
+int oshun_batch_set_tiles(oshun_batch b, int stage_threads, int tile_cells);
+int oshun_batch_get_tiles(oshun_batch b, int* stage_threads, int* tile_cells);
+/* Autotuner: times every tile candidate (stage threads 128/192/256 x cells
+ * per tile 1/2/4/8) on `steps` steps of the batch itself, keeps the fastest
+ * and restores the state and clocks; returns the choice and its ms/step. */
+int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile_cells, double* ms_per_step);
+
 /* ---- allocation-free collision step --------------------------------------- */
 
 /* No counterpart in the reference.  The implicit f_lm collision step (the work

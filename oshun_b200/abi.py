@@ -27,6 +27,9 @@ EXPORTED = [
     "oshun_download", "oshun_rhs", "oshun_rk4_step", "oshun_collide_ee", "oshun_collide_f1",
     "oshun_collide_flm", "oshun_step", "oshun_time", "oshun_status_flags", "oshun_device_state",
     "oshun_plane_index", "oshun_last_error", "oshun_abi_version", "oshun_collide_flm_noalloc",
+    "oshun_batch_create", "oshun_batch_destroy", "oshun_batch_size", "oshun_batch_problem",
+    "oshun_batch_upload", "oshun_batch_download", "oshun_batch_step", "oshun_batch_status",
+    "oshun_batch_set_tiles", "oshun_batch_get_tiles", "oshun_batch_autotune",
 ]
 
 
@@ -82,6 +85,18 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_plane_index.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.oshun_collide_flm_noalloc.argtypes = [ctypes.POINTER(OshunCfg), vp, vp, ctypes.c_double, vp,
                                               ctypes.POINTER(ctypes.c_longlong)]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.oshun_batch_create.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int, ip, ctypes.POINTER(vp)]
+    lib.oshun_batch_destroy.argtypes = [vp]
+    lib.oshun_batch_size.argtypes = [vp, ip]
+    lib.oshun_batch_problem.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+    lib.oshun_batch_upload.argtypes = [vp, ctypes.c_int, vp, vp]
+    lib.oshun_batch_download.argtypes = [vp, ctypes.c_int, vp, vp]
+    lib.oshun_batch_step.argtypes = [vp, ctypes.c_int]
+    lib.oshun_batch_status.argtypes = [vp, ip]
+    lib.oshun_batch_set_tiles.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.oshun_batch_get_tiles.argtypes = [vp, ip, ip]
+    lib.oshun_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ip, dp]
     lib.oshun_last_error.restype = ctypes.c_char_p
     lib.oshun_abi_version.restype = ctypes.c_int
     _lib = lib
@@ -203,3 +218,81 @@ class Handle:
         self._check(self.lib.oshun_device_state(self._h, ctypes.byref(f00), ctypes.byref(pl), ctypes.byref(fl),
                                                 ctypes.byref(pb), ctypes.byref(fb)), "oshun_device_state")
         return f00.value, pl.value, fl.value, pb.value, fb.value
+
+
+class Batch:
+    """One oshun_batch: independent problems advanced together, one captured
+    graph per step (see include/oshun_b200.h)."""
+
+    def __init__(self, cfgs, collide=None):
+        self.lib = load()
+        self.cfgs = [make_cfg(**c) for c in cfgs]
+        n = len(self.cfgs)
+        arr = (OshunCfg * n)(*self.cfgs)
+        col = None
+        if collide is not None:
+            col = (ctypes.c_int * n)(*[int(bool(x)) for x in collide])
+        self._b = ctypes.c_void_p()
+        self._check(self.lib.oshun_batch_create(arr, n, col, ctypes.byref(self._b)), "oshun_batch_create")
+        self.n = n
+        self.shapes = []
+        for c in self.cfgs:
+            nh = ((c.m0 + 1) * (2 * c.l0 - c.m0 + 2)) // 2
+            self.shapes.append(((nh, c.numy, c.numx, c.nump), (6, c.numy, c.numx)))
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            raise OshunError(rc, what, self.lib.oshun_last_error().decode())
+
+    def close(self) -> None:
+        if self._b:
+            self.lib.oshun_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, i: int, f: np.ndarray, fields: np.ndarray) -> None:
+        f = np.ascontiguousarray(f, np.complex128)
+        fields = np.ascontiguousarray(fields, np.complex128)
+        assert f.shape == self.shapes[i][0] and fields.shape == self.shapes[i][1]
+        self._check(self.lib.oshun_batch_upload(self._b, i, f.ctypes.data, fields.ctypes.data), "oshun_batch_upload")
+
+    def download(self, i: int):
+        f = np.empty(self.shapes[i][0], np.complex128)
+        fields = np.empty(self.shapes[i][1], np.complex128)
+        self._check(self.lib.oshun_batch_download(self._b, i, f.ctypes.data, fields.ctypes.data),
+                    "oshun_batch_download")
+        return f, fields
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self.lib.oshun_batch_step(self._b, nsteps), "oshun_batch_step")
+
+    def status(self) -> int:
+        f = ctypes.c_int()
+        self._check(self.lib.oshun_batch_status(self._b, ctypes.byref(f)), "oshun_batch_status")
+        return f.value
+
+    def set_tiles(self, stage_threads: int, tile_cells: int) -> None:
+        self._check(self.lib.oshun_batch_set_tiles(self._b, stage_threads, tile_cells), "oshun_batch_set_tiles")
+
+    def tiles(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.oshun_batch_get_tiles(self._b, ctypes.byref(a), ctypes.byref(b)), "oshun_batch_get_tiles")
+        return a.value, b.value
+
+    def autotune(self, steps: int = 2):
+        a, b, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self.lib.oshun_batch_autotune(self._b, steps, ctypes.byref(a), ctypes.byref(b), ctypes.byref(ms)),
+                    "oshun_batch_autotune")
+        return a.value, b.value, ms.value
+

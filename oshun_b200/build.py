@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "liboshun_b200.so")
-SOURCES = ["vlasov.cu", "stage_pipe.cu", "collide.cu", "abi.cu", "noalloc.cu"]
+SOURCES = ["vlasov.cu", "stage_pipe.cu", "stage_batch.cu", "collide.cu", "abi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -43,13 +43,20 @@ def build(verbose: bool = False, ptxas_info: bool = False, force: bool = False) 
                      "--expt-relaxed-constexpr", "-Xcompiler", "-Wall"]
     if ptxas_info:
         common += ["-Xptxas", "-v"]
-    objs = []
-    for src in SOURCES:
+    # translation units compile in parallel
+    def compile_one(src):
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
         cmd = [nvcc] + common + ["-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, r
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    objs = []
+    for src, obj, r in results:
         if r.returncode != 0 or (verbose and r.stderr):
             sys.stderr.write(r.stderr)
         if r.returncode != 0:

@@ -17,7 +17,9 @@
 // Y, Y0, Y1, Yh; def-RK.cpp:56): set `cur` is Y0 (stage-1 input), set `nxt`
 // is the accumulator Y that becomes the new state, sets 2 and 3 carry the
 // stage inputs.  `cur` and `nxt` swap after each step.
+#include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -164,6 +166,7 @@ struct oshun_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [parity][collisions]
+    bool graphs_ok = true;
 
     // host mirrors of the clocks (the reference's Runge_Kutta_4::t, Explicit_EC_FP::t, Euler_Backward::t)
     double t = 0.0, t_ee = 0.0, t_eb = 0.0;
@@ -424,7 +427,10 @@ int build_tables(oshun_ctx* h) {
 
     CK(cudaMalloc(&h->d_coef, sizeof(CoefLM) * coef.size()));
     CK(cudaMemcpy(h->d_coef, coef.data(), sizeof(CoefLM) * coef.size(), cudaMemcpyHostToDevice));
-    CK(cudaMalloc(&h->d_plane_of, sizeof(int) * plane_of.size()));
+    // padded to 16 bytes: batched launches bulk-copy the map
+    const size_t plane_bytes = (sizeof(int) * plane_of.size() + 15) / 16 * 16;
+    CK(cudaMalloc(&h->d_plane_of, plane_bytes));
+    CK(cudaMemset(h->d_plane_of, 0xff, plane_bytes));
     CK(cudaMemcpy(h->d_plane_of, plane_of.data(), sizeof(int) * plane_of.size(), cudaMemcpyHostToDevice));
     const size_t npl = std::max<size_t>(1, plane_l.size());
     CK(cudaMalloc(&h->d_plane_l, sizeof(int) * npl));
@@ -510,14 +516,38 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     return a;
 }
 
-int enqueue_collide(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt) {
-    CollideArgs a = collide_args(h, do_ee, do_l1, do_lm, nsub, hsub, Dt);
+int launch_collide_args(oshun_ctx* h, const CollideArgs& a) {
     cudaError_t e;
     if (h->tri_cpc > 0)
         e = launch_collide_tri(a, h->stream, h->tri_cpc, h->tri_blocks);
     else
         e = launch_collide(a, h->stream, h->collide_smem, h->collide_blocks);
     if (e != cudaSuccess) { set_error(std::string("collide launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+    return OSHUN_OK;
+}
+
+int enqueue_collide(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt) {
+    return launch_collide_args(h, collide_args(h, do_ee, do_l1, do_lm, nsub, hsub, Dt));
+}
+
+// One small step of the reference's main loop (main.cpp:77-107) on the device
+// clock, graph-capturable: RK4 on set cur, t += dt, then (collisions) the e-e
+// substeps and the implicit f1/f_lm solves with nsub, hsub, Dt from the
+// device clock, t_ee = t_eb = t.  Flips h->cur.
+int enqueue_step_device(oshun_ctx* h, int collisions) {
+    int rc = enqueue_rk4(h);
+    if (rc) return rc;
+    h->cur ^= 1;
+    clock_advance_kernel<<<1, 1, 0, h->stream>>>(h->d_clock, h->cfg.dt);
+    CK(cudaGetLastError());
+    if (collisions) {
+        CollideArgs a = collide_args(h, 1, 1, 1, 0, 0.0, 0.0);
+        a.clock = reinterpret_cast<const double*>(h->d_clock);
+        a.small_dt = h->cfg.small_dt;
+        if ((rc = launch_collide_args(h, a))) return rc;
+        clock_commit_kernel<<<1, 1, 0, h->stream>>>(h->d_clock, 1, 1);
+        CK(cudaGetLastError());
+    }
     return OSHUN_OK;
 }
 
@@ -641,6 +671,7 @@ int oshun_set_stream(oshun_handle h, void* stream) {
     for (int p = 0; p < 2; ++p)
         for (int c = 0; c < 2; ++c)
             if (h->graph[p][c]) { cudaGraphExecDestroy(h->graph[p][c]); h->graph[p][c] = nullptr; }
+    h->graphs_ok = true;
     if (stream) {
         h->stream = (cudaStream_t)stream;
     } else {
@@ -759,22 +790,42 @@ int oshun_collide_flm(oshun_handle h, double t_new) {
 
 int oshun_step(oshun_handle h, int nsteps, int collisions) {
     if (!h || nsteps < 0) return OSHUN_ERR_ARG;
+    collisions = collisions ? 1 : 0;
+    Clock ck{h->t, h->t_ee, h->t_eb};
+    CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
     for (int s = 0; s < nsteps; ++s) {
-        int rc = enqueue_rk4(h);
-        if (rc) return rc;
-        h->cur ^= 1;
+        // one graph per state parity: RK4 stages, clocks, collision step
+        cudaGraphExec_t& g = h->graph[h->cur][collisions];
+        if (!g && h->graphs_ok) {
+            const int cur0 = h->cur;
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            int rc = ok ? enqueue_step_device(h, collisions) : OSHUN_OK;
+            h->cur = cur0;
+            if (ok) ok = cudaStreamEndCapture(h->stream, &graph) == cudaSuccess && rc == OSHUN_OK;
+            if (ok) ok = cudaGraphInstantiate(&g, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            if (!ok) {
+                // capture unavailable on this stream: plain launches from now on
+                (void)cudaGetLastError();
+                if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+                h->graphs_ok = false;
+                if (rc) return rc;
+            }
+        }
+        if (g) {
+            CK(cudaGraphLaunch(g, h->stream));
+            h->cur ^= 1;
+        } else {
+            int rc = enqueue_step_device(h, collisions);
+            if (rc) return rc;
+        }
         h->t += h->cfg.dt;
         if (collisions) {
-            int nsub; double hsub, Dt;
-            collide_params(h, h->t, &nsub, &hsub, &Dt);
-            rc = enqueue_collide(h, 1, 1, 1, nsub, hsub, Dt);
-            if (rc) return rc;
             h->t_ee = h->t;
             h->t_eb = h->t;
         }
     }
-    Clock ck{h->t, h->t_ee, h->t_eb};
-    CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return OSHUN_OK;
 }
@@ -819,6 +870,536 @@ int oshun_plane_index(oshun_handle h, int l, int m, int* plane) {
             q += mm > 0 ? 2 : 1;
         }
     return OSHUN_ERR_ARG;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches of independent problems (no counterpart in the reference, whose
+// runs are one problem per process): every problem keeps its own handle
+// (state sets, tables, clocks); one step of the batch is one captured graph of
+//   4 x batched RK4 stage launch (one persistent kernel each, over the
+//       (problem, tile) list of the whole batch),
+//   device clock advance,
+//   per group of problems with equal ceil(nump/32): one batched collision
+//       launch over their (problem, cell) list,
+//   device clock commit.
+// The stage tiles (consumer threads per CTA, cells per tile) are chosen by
+// oshun_batch_autotune, which times each candidate on the batch itself.
+// ---------------------------------------------------------------------------
+struct oshun_batch_ctx {
+    std::vector<oshun_ctx*> P;
+    std::vector<int> collide;       // per problem: collision step on
+    bool fp32 = false;
+    int mc = 0;                     // template class of the largest m0
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int cur = 0;                    // parity of every problem's state sets
+    int nc = 192, tx_cap = 8;       // stage tiles
+    // stage launches
+    int desc_bytes = 0, ncoef_max = 0, hdr_bytes = 0;
+    unsigned char* d_desc = nullptr;   // [2 parities][4 stages][n] descriptors
+    void* d_coef_ts = nullptr;         // coupling tables in the arithmetic type
+    int2* d_items = nullptr;
+    int nitems = 0;
+    size_t slot_bytes = 0, row_arr_bytes = 0;
+    std::vector<unsigned char> h_a1[2][4];   // kernel parameter of each launch (a problem's descriptor)
+    // collision launches
+    struct Group {
+        int E = 0;
+        size_t smem = 0;
+        CollideArgs* d_args[2] = {nullptr, nullptr};   // per parity
+        int2* d_items = nullptr;
+        long long nitems = 0;
+    };
+    std::vector<Group> groups;
+    double* d_clocks = nullptr;   // [n][t, t_ee, t_eb]
+    double* d_dt = nullptr;       // [n]
+    int* d_collide = nullptr;     // [n]
+    int* d_status = nullptr;      // pipeline status of the batched launches
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graphs_ok = true;
+};
+
+namespace {
+
+void batch_drop_graphs(oshun_batch_ctx* b) {
+    for (int c = 0; c < 2; ++c)
+        if (b->graph[c]) { cudaGraphExecDestroy(b->graph[c]); b->graph[c] = nullptr; }
+}
+
+void free_batch(oshun_batch_ctx* b) {
+    batch_drop_graphs(b);
+    for (oshun_ctx* h : b->P)
+        if (h) free_ctx(h);
+    for (auto& g : b->groups) { cudaFree(g.d_args[0]); cudaFree(g.d_args[1]); cudaFree(g.d_items); }
+    cudaFree(b->d_desc); cudaFree(b->d_coef_ts); cudaFree(b->d_items);
+    cudaFree(b->d_clocks); cudaFree(b->d_dt); cudaFree(b->d_collide); cudaFree(b->d_status);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+// descriptor of RK4 stage k (Runge_Kutta_4::advance_p1, def-RK.cpp:116-142)
+// of problem h for state parity c, as launch_stage builds it
+template <typename TS>
+StageArgs<TS> batch_stage_args(const oshun_ctx* h, int c, int k, const void* coef_ts) {
+    const double dt = h->cfg.dt;
+    const int B = c, A = c ^ 1, Sa = 2, Sb = 3;
+    const int in_set[4] = {B, Sa, Sb, Sa}, out_set[4] = {Sa, Sb, Sa, -1};
+    const double c1[4] = {0.5 * dt, 0.5 * dt, dt, dt / 6.0}, c2[4] = {1.0 / 3.0, 2.0 / 3.0, 1.0 / 3.0, 1.0};
+    StageArgs<TS> a = h->stage_args<TS>(in_set[k], out_set[k], 0);
+    a.f00_B = h->f00[B]; a.pl_B = (const TS*)h->pl[B]; a.fld_B = (const TS*)h->fld[B];
+    a.f00_A = h->f00[A]; a.pl_A = (TS*)h->pl[A]; a.fld_A = (TS*)h->fld[A];
+    if (out_set[k] >= 0) {
+        a.f00_out = h->f00[out_set[k]]; a.pl_out = (TS*)h->pl[out_set[k]]; a.fld_out = (TS*)h->fld[out_set[k]];
+    }
+    a.first = k == 0; a.c1 = c1[k]; a.c2 = c2[k];
+    a.coef_ts = coef_ts;
+    return a;
+}
+
+// (problem, tile) list for the current tiles, heaviest tiles first, so that
+// the persistent CTAs' round-robin shares are even
+int batch_build_items(oshun_batch_ctx* b) {
+    const int esz = b->fp32 ? 4 : 8;
+    struct It { double cost; int p, tile; };
+    std::vector<It> items;
+    size_t slot = 0, rowb = 0;
+    for (int i = 0; i < (int)b->P.size(); ++i) {
+        const oshun_cfg& c = b->P[i]->cfg;
+        if (((c.nump + 31) / 32) * 32 > b->nc) {
+            set_error("batch stage threads below a problem's padded nump");
+            return OSHUN_ERR_UNSUPPORTED;
+        }
+        int tx;
+        size_t sb, rb;
+        stage_batch_sizes(c.nump, c.numx, c.numy, c.l0, c.m0, b->nc, b->tx_cap, esz, &tx, &sb, &rb);
+        slot = std::max(slot, sb);
+        rowb = std::max(rowb, rb);
+        const int tiles = c.numy * ((c.numx + tx - 1) / tx);
+        const double cost = (double)b->P[i]->nh * (double)(((c.nump + 31) / 32) * 32) * tx;
+        for (int t = 0; t < tiles; ++t) items.push_back({cost, i, t});
+    }
+    BatchWork bw{};
+    bw.hdr_bytes = b->hdr_bytes; bw.slot_bytes = (int)slot; bw.row_arr_bytes = (int)rowb;
+    if (stage_batch_smem(bw, esz) > 227 * 1024) {
+        set_error("batch tiles do not fit in shared memory (lower the cells per tile)");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
+    std::stable_sort(items.begin(), items.end(), [](const It& x, const It& y) { return x.cost > y.cost; });
+    std::vector<int2> h(items.size());
+    for (size_t k = 0; k < items.size(); ++k) h[k] = make_int2(items[k].p, items[k].tile);
+    cudaFree(b->d_items);
+    b->d_items = nullptr;
+    CK(cudaMalloc(&b->d_items, sizeof(int2) * std::max<size_t>(1, h.size())));
+    CK(cudaMemcpy(b->d_items, h.data(), sizeof(int2) * h.size(), cudaMemcpyHostToDevice));
+    b->nitems = (int)h.size();
+    b->slot_bytes = slot;
+    b->row_arr_bytes = rowb;
+    return OSHUN_OK;
+}
+
+BatchWork batch_work(const oshun_batch_ctx* b, int c, int k) {
+    BatchWork bw{};
+    bw.probs = b->d_desc + ((size_t)(c * 4 + k) * b->P.size()) * b->desc_bytes;
+    bw.items = b->d_items;
+    bw.nitems = b->nitems;
+    bw.tx_cap = b->tx_cap;
+    bw.desc_bytes = b->desc_bytes;
+    bw.ncoef_max = b->ncoef_max;
+    bw.hdr_bytes = b->hdr_bytes;
+    bw.slot_bytes = (int)b->slot_bytes;
+    bw.row_arr_bytes = (int)b->row_arr_bytes;
+    return bw;
+}
+
+// one step of every problem for state parity c (graph-capturable)
+int batch_enqueue_step(oshun_batch_ctx* b, int c) {
+    const int n = (int)b->P.size();
+    for (int k = 0; k < 4; ++k) {
+        const BatchWork bw = batch_work(b, c, k);
+        cudaError_t e;
+        if (b->fp32)
+            e = launch_stage_batch<float>(*reinterpret_cast<const StageArgs<float>*>(b->h_a1[c][k].data()), bw, b->mc,
+                                          b->nc, b->stream);
+        else
+            e = launch_stage_batch<double>(*reinterpret_cast<const StageArgs<double>*>(b->h_a1[c][k].data()), bw,
+                                           b->mc, b->nc, b->stream);
+        if (e != cudaSuccess) { set_error(std::string("batched stage launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+    }
+    CK(launch_clock_advance(b->d_clocks, b->d_dt, n, b->stream));
+    for (const auto& g : b->groups) {
+        CollideBatch cb{g.d_args[c ^ 1], g.d_items, g.nitems};   // the new state is parity c^1
+        cudaError_t e = launch_collide_batch(cb, g.E, b->fp32 ? 1 : 0, g.smem, b->stream);
+        if (e != cudaSuccess) { set_error(std::string("batched collision launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+    }
+    CK(launch_clock_commit(b->d_clocks, b->d_collide, n, b->stream));
+    return OSHUN_OK;
+}
+
+int batch_upload_clocks(oshun_batch_ctx* b) {
+    std::vector<double> ck(3 * b->P.size());
+    for (size_t i = 0; i < b->P.size(); ++i) {
+        ck[3 * i] = b->P[i]->t; ck[3 * i + 1] = b->P[i]->t_ee; ck[3 * i + 2] = b->P[i]->t_eb;
+    }
+    CK(cudaMemcpyAsync(b->d_clocks, ck.data(), sizeof(double) * ck.size(), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return OSHUN_OK;
+}
+
+// host mirrors of the clocks after one step (the same arithmetic as the device)
+void batch_advance_host(oshun_batch_ctx* b) {
+    b->cur ^= 1;
+    for (size_t i = 0; i < b->P.size(); ++i) {
+        oshun_ctx* h = b->P[i];
+        h->cur = b->cur;
+        h->t += h->cfg.dt;
+        if (b->collide[i]) { h->t_ee = h->t; h->t_eb = h->t; }
+    }
+}
+
+int batch_steps_plain(oshun_batch_ctx* b, int nsteps) {
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = batch_enqueue_step(b, b->cur);
+        if (rc) return rc;
+        batch_advance_host(b);
+    }
+    return OSHUN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_batch* out) {
+    if (!out || !cfgs || n < 1) { set_error("bad batch arguments"); return OSHUN_ERR_ARG; }
+    *out = nullptr;
+    oshun_batch_ctx* b = new oshun_batch_ctx();
+    auto fail = [&](int code) { free_batch(b); return code; };
+#define CKB(call)                                                                  \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+            return fail(OSHUN_ERR_CUDA);                                           \
+        }                                                                          \
+    } while (0)
+    b->fp32 = cfgs[0].precision == OSHUN_FP32_SPLIT;
+    CKB(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->own_stream = true;
+    const int esz = b->fp32 ? 4 : 8;
+    int m0max = 0;
+    for (int i = 0; i < n; ++i) {
+        const oshun_cfg& c = cfgs[i];
+        if (c.precision != cfgs[0].precision) { set_error("a batch has one precision"); return fail(OSHUN_ERR_ARG); }
+        if (((c.nump + 31) / 32) * 32 > 256 || (c.nump * esz) % 16 != 0) {
+            set_error("batched problems need nump <= 256 with nump * element size a multiple of 16 bytes");
+            return fail(OSHUN_ERR_UNSUPPORTED);
+        }
+        const int col = collide ? (collide[i] != 0) : 1;
+        if (col && !c.if_tridiagonal) { set_error("batched collision steps are tridiagonal"); return fail(OSHUN_ERR_UNSUPPORTED); }
+        oshun_handle h = nullptr;
+        int rc = oshun_create(&c, &h);
+        if (rc) return fail(rc);
+        b->P.push_back(h);
+        b->collide.push_back(col);
+        if ((rc = oshun_set_stream(h, b->stream))) return fail(rc);
+        m0max = std::max(m0max, c.m0);
+        b->ncoef_max = std::max(b->ncoef_max, (c.l0 + 1) * (c.m0 + 1));
+    }
+    b->mc = pick_mc(m0max);
+    b->desc_bytes = (int)((std::max(sizeof(StageArgs<float>), sizeof(StageArgs<double>)) + 15) / 16 * 16);
+    const int cbytes = stage_batch_coef_bytes(esz);
+    b->hdr_bytes = b->desc_bytes + cbytes * b->ncoef_max + (int)((sizeof(int) * b->ncoef_max + 15) / 16 * 16);
+
+    // coupling tables in the arithmetic type
+    std::vector<size_t> coff(n);
+    size_t ctot = 0;
+    for (int i = 0; i < n; ++i) {
+        coff[i] = ctot;
+        ctot += (size_t)cbytes * (b->P[i]->cfg.l0 + 1) * (b->P[i]->cfg.m0 + 1);
+    }
+    CKB(cudaMalloc(&b->d_coef_ts, ctot));
+    {
+        std::vector<unsigned char> hc(ctot);
+        for (int i = 0; i < n; ++i) {
+            const int nco = (b->P[i]->cfg.l0 + 1) * (b->P[i]->cfg.m0 + 1);
+            std::vector<double> dc((size_t)nco * 16);
+            CKB(cudaMemcpy(dc.data(), b->P[i]->d_coef, sizeof(double) * dc.size(), cudaMemcpyDeviceToHost));
+            for (size_t k = 0; k < dc.size(); ++k) {
+                if (b->fp32) { const float v = (float)dc[k]; std::memcpy(&hc[coff[i] + 4 * k], &v, 4); }
+                else std::memcpy(&hc[coff[i] + 8 * k], &dc[k], 8);
+            }
+        }
+        CKB(cudaMemcpy(b->d_coef_ts, hc.data(), ctot, cudaMemcpyHostToDevice));
+    }
+    // stage descriptors [parity][stage][problem] and the launches' parameters
+    CKB(cudaMalloc(&b->d_status, sizeof(int) * 4));
+    CKB(cudaMemset(b->d_status, 0, sizeof(int) * 4));
+    {
+        std::vector<unsigned char> hd((size_t)8 * n * b->desc_bytes, 0);
+        for (int c = 0; c < 2; ++c)
+            for (int k = 0; k < 4; ++k)
+                for (int i = 0; i < n; ++i) {
+                    unsigned char* dst = &hd[((size_t)(c * 4 + k) * n + i) * b->desc_bytes];
+                    const void* ct = (const unsigned char*)b->d_coef_ts + coff[i];
+                    if (b->fp32) {
+                        StageArgs<float> a = batch_stage_args<float>(b->P[i], c, k, ct);
+                        std::memcpy(dst, &a, sizeof(a));
+                    } else {
+                        StageArgs<double> a = batch_stage_args<double>(b->P[i], c, k, ct);
+                        std::memcpy(dst, &a, sizeof(a));
+                    }
+                    if (i == 0) {
+                        b->h_a1[c][k].assign(dst, dst + b->desc_bytes);
+                        // pipeline timeouts of a batched launch land in the batch's status word
+                        int* st = b->d_status;
+                        const size_t off = b->fp32 ? offsetof(StageArgs<float>, err) : offsetof(StageArgs<double>, err);
+                        std::memcpy(b->h_a1[c][k].data() + off, &st, sizeof(st));
+                    }
+                }
+        CKB(cudaMalloc(&b->d_desc, hd.size()));
+        CKB(cudaMemcpy(b->d_desc, hd.data(), hd.size(), cudaMemcpyHostToDevice));
+    }
+    // default tiles: 192 consumer threads, or 256 when a momentum row needs them
+    int pad_max = 32;
+    for (oshun_ctx* h : b->P) pad_max = std::max(pad_max, ((h->cfg.nump + 31) / 32) * 32);
+    b->nc = pad_max <= 192 ? 192 : 256;
+    b->tx_cap = 8;
+    int rc = batch_build_items(b);
+    if (rc) return fail(rc);
+    // device clocks and per-problem steps
+    CKB(cudaMalloc(&b->d_clocks, sizeof(double) * 3 * n));
+    CKB(cudaMalloc(&b->d_dt, sizeof(double) * n));
+    CKB(cudaMalloc(&b->d_collide, sizeof(int) * n));
+    {
+        std::vector<double> dt(n);
+        for (int i = 0; i < n; ++i) dt[i] = b->P[i]->cfg.dt;
+        CKB(cudaMemcpy(b->d_dt, dt.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        CKB(cudaMemcpy(b->d_collide, b->collide.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
+    // collision groups by ceil(nump / 32): descriptors per state parity, (problem, cell) items
+    for (int E = 1; E <= 8; ++E) {
+        oshun_batch_ctx::Group g;
+        g.E = E;
+        std::vector<CollideArgs> args[2];
+        std::vector<int2> items;
+        for (int i = 0; i < n; ++i) {
+            oshun_ctx* h = b->P[i];
+            if (!b->collide[i] || (h->cfg.nump + 31) / 32 != E) continue;
+            const int local = (int)args[0].size();
+            for (int c = 0; c < 2; ++c) {
+                const int cur0 = h->cur;
+                h->cur = c;
+                CollideArgs a = collide_args(h, 1, 1, 1, 0, 0.0, 0.0);
+                h->cur = cur0;
+                a.clock = b->d_clocks + 3 * i;
+                a.small_dt = h->cfg.small_dt;
+                args[c].push_back(a);
+            }
+            g.smem = std::max(g.smem, collide_tri_smem_per_cell(h->cfg.nump, h->cfg.l0));
+            for (long long cell = 0; cell < h->cells; ++cell) items.push_back(make_int2(local, (int)cell));
+        }
+        if (items.empty()) continue;
+        b->groups.push_back(g);
+        auto& gg = b->groups.back();
+        gg.nitems = (long long)items.size();
+        for (int c = 0; c < 2; ++c) {
+            CKB(cudaMalloc(&gg.d_args[c], sizeof(CollideArgs) * args[c].size()));
+            CKB(cudaMemcpy(gg.d_args[c], args[c].data(), sizeof(CollideArgs) * args[c].size(), cudaMemcpyHostToDevice));
+        }
+        CKB(cudaMalloc(&gg.d_items, sizeof(int2) * items.size()));
+        CKB(cudaMemcpy(gg.d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
+    }
+#undef CKB
+    if ((rc = batch_upload_clocks(b))) return fail(rc);
+    *out = b;
+    return OSHUN_OK;
+}
+
+int oshun_batch_destroy(oshun_batch b) {
+    if (!b) return OSHUN_ERR_ARG;
+    cudaStreamSynchronize(b->stream);
+    free_batch(b);
+    return OSHUN_OK;
+}
+
+int oshun_batch_size(oshun_batch b, int* n) {
+    if (!b || !n) return OSHUN_ERR_ARG;
+    *n = (int)b->P.size();
+    return OSHUN_OK;
+}
+
+int oshun_batch_problem(oshun_batch b, int i, oshun_handle* h) {
+    if (!b || !h || i < 0 || i >= (int)b->P.size()) return OSHUN_ERR_ARG;
+    *h = b->P[i];
+    return OSHUN_OK;
+}
+
+int oshun_batch_upload(oshun_batch b, int i, const double* harmonics, const double* fields) {
+    if (!b || i < 0 || i >= (int)b->P.size()) return OSHUN_ERR_ARG;
+    return oshun_upload(b->P[i], harmonics, fields);
+}
+
+int oshun_batch_download(oshun_batch b, int i, double* harmonics, double* fields) {
+    if (!b || i < 0 || i >= (int)b->P.size()) return OSHUN_ERR_ARG;
+    return oshun_download(b->P[i], harmonics, fields);
+}
+
+int oshun_batch_set_tiles(oshun_batch b, int stage_threads, int tile_cells) {
+    if (!b || stage_threads < 32 || stage_threads > 256 || stage_threads % 32 || tile_cells < 1 || tile_cells > 8)
+        return OSHUN_ERR_ARG;
+    CK(cudaStreamSynchronize(b->stream));
+    const int nc0 = b->nc, tx0 = b->tx_cap;
+    b->nc = stage_threads;
+    b->tx_cap = tile_cells;
+    int rc = batch_build_items(b);
+    if (rc) {
+        const std::string why = g_last_error;
+        b->nc = nc0; b->tx_cap = tx0;
+        batch_build_items(b);
+        set_error(why);
+        return rc;
+    }
+    batch_drop_graphs(b);
+    return OSHUN_OK;
+}
+
+int oshun_batch_get_tiles(oshun_batch b, int* stage_threads, int* tile_cells) {
+    if (!b) return OSHUN_ERR_ARG;
+    if (stage_threads) *stage_threads = b->nc;
+    if (tile_cells) *tile_cells = b->tx_cap;
+    return OSHUN_OK;
+}
+
+int oshun_batch_step(oshun_batch b, int nsteps) {
+    if (!b || nsteps < 0) return OSHUN_ERR_ARG;
+    int rc = batch_upload_clocks(b);
+    if (rc) return rc;
+    for (int s = 0; s < nsteps; ++s) {
+        cudaGraphExec_t& g = b->graph[b->cur];
+        if (!g && b->graphs_ok) {
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            rc = ok ? batch_enqueue_step(b, b->cur) : OSHUN_OK;
+            if (ok) ok = cudaStreamEndCapture(b->stream, &graph) == cudaSuccess && rc == OSHUN_OK;
+            if (ok) ok = cudaGraphInstantiate(&g, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            if (!ok) {
+                (void)cudaGetLastError();
+                if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+                b->graphs_ok = false;
+                if (rc) return rc;
+            }
+        }
+        if (g) {
+            CK(cudaGraphLaunch(g, b->stream));
+            batch_advance_host(b);
+        } else if ((rc = batch_steps_plain(b, 1))) {
+            return rc;
+        }
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    return OSHUN_OK;
+}
+
+int oshun_batch_status(oshun_batch b, int* flags) {
+    if (!b) return OSHUN_ERR_ARG;
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    int any = st;
+    for (oshun_ctx* h : b->P) {
+        int f = 0;
+        int rc = oshun_status_flags(h, &f, nullptr);
+        if (rc) return rc;
+        any |= f;
+    }
+    if (flags) *flags = any;
+    return OSHUN_OK;
+}
+
+// Times every stage tiling candidate -- consumer threads per CTA x cells per
+// tile -- on `steps` steps of the batch itself (after one untimed step) and
+// keeps the fastest.  The state and the clocks are restored after each trial.
+int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile_cells, double* ms_per_step) {
+    if (!b || steps < 1) return OSHUN_ERR_ARG;
+    CK(cudaStreamSynchronize(b->stream));
+    const int n = (int)b->P.size();
+    std::vector<void*> bak(3 * n, nullptr);
+    int rc = OSHUN_OK;
+    // copy every problem's current set to (save) or from (restore) the backup
+    auto save_restore = [&](bool save) -> int {
+        for (int i = 0; i < n; ++i) {
+            oshun_ctx* h = b->P[i];
+            void* live[3] = {h->f00[b->cur], h->pl[b->cur], h->fld[b->cur]};
+            const size_t sz[3] = {sizeof(double) * h->pstride,
+                                  h->ts * std::max<long long>(1, (long long)h->nplanes * h->pstride),
+                                  h->ts * 6 * h->cells};
+            for (int k = 0; k < 3; ++k) {
+                if (save) {
+                    if (!bak[3 * i + k]) CK(cudaMalloc(&bak[3 * i + k], sz[k]));
+                    CK(cudaMemcpyAsync(bak[3 * i + k], live[k], sz[k], cudaMemcpyDeviceToDevice, b->stream));
+                } else {
+                    CK(cudaMemcpyAsync(live[k], bak[3 * i + k], sz[k], cudaMemcpyDeviceToDevice, b->stream));
+                }
+            }
+        }
+        return OSHUN_OK;
+    };
+    const int cur0 = b->cur;
+    std::vector<double> t0(n), tee0(n), teb0(n);
+    for (int i = 0; i < n; ++i) { t0[i] = b->P[i]->t; tee0[i] = b->P[i]->t_ee; teb0[i] = b->P[i]->t_eb; }
+    auto reset_clocks = [&]() {
+        b->cur = cur0;
+        for (int i = 0; i < n; ++i) {
+            b->P[i]->cur = cur0; b->P[i]->t = t0[i]; b->P[i]->t_ee = tee0[i]; b->P[i]->t_eb = teb0[i];
+        }
+        return batch_upload_clocks(b);
+    };
+    rc = save_restore(true);
+    if (!rc) {
+        const int nc_c[] = {128, 192, 256};
+        const int tx_c[] = {1, 2, 4, 8};
+        int best_nc = b->nc, best_tx = b->tx_cap;
+        double best = 1e300;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        for (int nc : nc_c) {
+            for (int tx : tx_c) {
+                b->nc = nc;
+                b->tx_cap = tx;
+                if (batch_build_items(b) != OSHUN_OK) { (void)cudaGetLastError(); continue; }
+                if ((rc = batch_steps_plain(b, 1))) break;
+                cudaEventRecord(e0, b->stream);
+                if ((rc = batch_steps_plain(b, steps))) break;
+                cudaEventRecord(e1, b->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms / steps < best) { best = ms / steps; best_nc = nc; best_tx = tx; }
+                if ((rc = save_restore(false))) break;
+                if ((rc = reset_clocks())) break;
+            }
+            if (rc) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->nc = best_nc;
+        b->tx_cap = best_tx;
+        const int rc2 = batch_build_items(b);
+        if (!rc) rc = rc2;
+        if (!rc) rc = save_restore(false);
+        if (!rc) rc = reset_clocks();
+        batch_drop_graphs(b);
+        if (stage_threads) *stage_threads = best_nc;
+        if (tile_cells) *tile_cells = best_tx;
+        if (ms_per_step) *ms_per_step = best;
+    }
+    cudaStreamSynchronize(b->stream);
+    for (void* p : bak) cudaFree(p);
+    return rc;
 }
 
 }  // extern "C"

@@ -466,7 +466,20 @@ __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
     }
 }
 
-__global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideArgs a) {
+// the reference's clock arithmetic for one collision step ending at the
+// device clock's t (Explicit_EC_FP::loop, def-FokkerPlanck.cpp:598-599;
+// Euler_Backward, :1277, 1297), as collide_params does on the host
+__device__ __forceinline__ void apply_clock(CollideArgs& a) {
+    if (!a.clock) return;
+    const double t = a.clock[0], t_ee = a.clock[1], t_eb = a.clock[2];
+    a.nsub = (int)((t - t_ee) / a.small_dt) + 1;
+    a.hsub = (t - t_ee) / (double)a.nsub;
+    a.Dt = t - t_eb;
+}
+
+__global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideArgs a0) {
+    CollideArgs a = a0;
+    apply_clock(a);
     extern __shared__ double smem[];
     const int n = a.np;
     Smem s = carve(smem, n);
@@ -512,7 +525,9 @@ __device__ __forceinline__ bool collided(const CollideArgs& a, int l, int m) {
 //      d'_i = (d_i - a_i d'_{i-1}) id_i (forward) and x_i = d'_i - c'_i x_{i+1}
 //      (backward); inside the run the lane applies the reference's recursion.
 template <typename TP>
-__global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
+__global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a0) {
+    CollideArgs a = a0;
+    apply_clock(a);
     extern __shared__ double smem[];
     const int n = a.np;
     const int l0 = a.l0;
@@ -650,8 +665,7 @@ __host__ __device__ inline size_t lane_smem_doubles(int np, int l0) {
 }
 
 template <typename TP, int E, int P>
-__global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
-    extern __shared__ double smem[];
+__device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const long long cell, double* smem) {
     const int n = a.np;
     const int l0 = a.l0;
     const int lane = threadIdx.x & 31;
@@ -686,7 +700,7 @@ __global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
     };
 
     double cur[P][E], nxt[P][E];
-    for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) {
+    {
         int bl, bj;
         batch_first(bl, bj);
         if (solve) load_batch(cell, bl, bj, cur);   // in flight during the e-e step
@@ -696,7 +710,7 @@ __global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
             ee_substeps(a, s);
             for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
         }
-        if (!solve) continue;
+        if (!solve) return;
         flm_reset(a, s, s.f);
         // pivots of every collided l, one lane per l
         for (int l = 1 + lane; l <= l0; l += 32) {
@@ -834,6 +848,27 @@ __global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
     }
 }
 
+template <typename TP, int E, int P>
+__global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a0) {
+    extern __shared__ double smem[];
+    CollideArgs a = a0;
+    apply_clock(a);
+    for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) collide_lane_cell<TP, E, P>(a, cell, smem);
+}
+
+// batched form: work item = (problem, cell); the problems share E
+template <typename TP, int E, int P>
+__global__ void __launch_bounds__(32) collide_lane_batch_kernel(const CollideBatch b) {
+    extern __shared__ double smem[];
+    for (long long it = blockIdx.x; it < b.nitems; it += gridDim.x) {
+        const int2 w = b.items[it];
+        CollideArgs a = b.probs[w.x];
+        apply_clock(a);
+        collide_lane_cell<TP, E, P>(a, (long long)w.y, smem);
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
 size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal) {
@@ -899,6 +934,60 @@ cudaError_t launch_lane_e(const CollideArgs& a, cudaStream_t st, int blocks, siz
     }
 }
 }  // namespace
+
+namespace {
+template <typename TP, int E>
+cudaError_t launch_lane_batch(const CollideBatch& b, cudaStream_t st, size_t smem) {
+    constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
+    static size_t attr = 0;
+    if (smem > attr) {
+        cudaError_t e = cudaFuncSetAttribute(collide_lane_batch_kernel<TP, E, P>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = smem;
+    }
+    const long long blocks = b.nitems < (1ll << 30) ? b.nitems : (1ll << 30);
+    if (blocks < 1) return cudaSuccess;
+    collide_lane_batch_kernel<TP, E, P><<<(unsigned)blocks, 32, smem, st>>>(b);
+    return cudaGetLastError();
+}
+template <typename TP>
+cudaError_t launch_lane_batch_e(const CollideBatch& b, int E, cudaStream_t st, size_t smem) {
+    switch (E) {
+        case 1: return launch_lane_batch<TP, 1>(b, st, smem);
+        case 2: return launch_lane_batch<TP, 2>(b, st, smem);
+        case 3: return launch_lane_batch<TP, 3>(b, st, smem);
+        case 4: return launch_lane_batch<TP, 4>(b, st, smem);
+        case 5: return launch_lane_batch<TP, 5>(b, st, smem);
+        case 6: return launch_lane_batch<TP, 6>(b, st, smem);
+        case 7: return launch_lane_batch<TP, 7>(b, st, smem);
+        case 8: return launch_lane_batch<TP, 8>(b, st, smem);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+__global__ void clock_advance_batch_kernel(double* clocks, const double* dt, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) clocks[3 * i] += dt[i];
+}
+__global__ void clock_commit_batch_kernel(double* clocks, const int* collide, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && (!collide || collide[i])) { clocks[3 * i + 1] = clocks[3 * i]; clocks[3 * i + 2] = clocks[3 * i]; }
+}
+}  // namespace
+
+cudaError_t launch_collide_batch(const CollideBatch& b, int E, int planes_fp32, size_t smem, cudaStream_t st) {
+    if (planes_fp32) return launch_lane_batch_e<float>(b, E, st, smem);
+    return launch_lane_batch_e<double>(b, E, st, smem);
+}
+cudaError_t launch_clock_advance(double* clocks, const double* dt, int n, cudaStream_t st) {
+    clock_advance_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(clocks, dt, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_clock_commit(double* clocks, const int* collide, int n, cudaStream_t st) {
+    clock_commit_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(clocks, collide, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_collide_tri(const CollideArgs& a, cudaStream_t st, int /*cells_per_cta*/, int blocks) {
     const size_t smem = collide_tri_smem_per_cell(a.np, a.l0);

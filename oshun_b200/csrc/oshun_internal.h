@@ -60,6 +60,7 @@ struct StageArgs {
     const int* seq;       // [nh]: source harmonics in stream order, s | (m << 16)
     int nh;
     int* err;             // error word (bit 4: a pipeline wait timed out)
+    const void* coef_ts;  // coupling table in the arithmetic type (batched launches)
 };
 
 struct CollideArgs {
@@ -85,6 +86,17 @@ struct CollideArgs {
     int chunk;            // planes staged per pass (tridiagonal path)
     double* dense_ws;     // dense path: np*np doubles per block
     int* status;          // [0] flags, [1] non-dominant count
+    // when set, nsub/hsub/Dt come from this device clock {t, t_ee, t_eb} at
+    // kernel start (the reference's clock arithmetic, see collide_params)
+    const double* clock;
+    double small_dt;
+};
+
+// batched collision launch: CollideArgs per problem, (problem, cell) work items
+struct CollideBatch {
+    const CollideArgs* probs;
+    const int2* items;
+    long long nitems;
 };
 
 // launchers (return cudaError_t)
@@ -92,12 +104,39 @@ struct CollideArgs {
 template <typename TS>
 cudaError_t launch_stage_pipe(const StageArgs<TS>& a, int mc, cudaStream_t s);
 cudaError_t launch_stage_fp64(const StageArgs<double>& a, int mc, cudaStream_t s);
+// The work of one stage launch: a list of tiles, either of one problem (the
+// kernel parameter) or of a batch of problems (`probs` holds one StageArgs per
+// problem, `items` the (problem, tile) pairs).  In a batch the first bulk copy
+// of each tile also brings the problem's descriptor, its coupling table and
+// its plane map into the slot's header.
+struct BatchWork {
+    const unsigned char* probs;   // StageArgs<TS>[nprob], desc_bytes apart
+    const int2* items;            // (problem, tile)
+    int nitems;
+    int tx_cap;                   // cells per tile at most
+    int desc_bytes;               // sizeof(StageArgs<TS>) rounded to 16
+    int ncoef_max;                // largest (l0+1)(m0+1) of the batch
+    int hdr_bytes;                // descriptor + coupling table + plane map
+    int slot_bytes, row_arr_bytes;   // largest slot / staged-row array of the batch
+};
+// batched stage kernel (stage_batch.cu); nc consumer threads per CTA
+template <typename TS>
+cudaError_t launch_stage_batch(const StageArgs<TS>& a1, const BatchWork& bw, int mc, int nc, cudaStream_t s);
+size_t stage_batch_smem(const BatchWork& bw, int elem_bytes);
+void stage_batch_sizes(int np, int nx, int ny, int l0, int m0, int nc, int tx_cap, int elem_bytes, int* tx,
+                       size_t* slot_bytes, size_t* row_arr_bytes);
+int stage_batch_coef_bytes(int elem_bytes);
 cudaError_t launch_stage_fp32(const StageArgs<float>& a, int mc, cudaStream_t s);
 cudaError_t launch_collide(const CollideArgs& a, cudaStream_t s, size_t smem_bytes, int blocks);
 size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal);
 int collide_max_chunk(int np, size_t smem_budget);
 int collide_threads();
 size_t collide_tri_smem_per_cell(int np, int l0);
+// tridiagonal collision step of a batch whose problems share E = ceil(np/32) <= 8
+cudaError_t launch_collide_batch(const CollideBatch& b, int E, int planes_fp32, size_t smem, cudaStream_t s);
+// device clocks {t, t_ee, t_eb} of n problems: t += dt; after a collision step t_ee = t_eb = t
+cudaError_t launch_clock_advance(double* clocks, const double* dt, int n, cudaStream_t s);
+cudaError_t launch_clock_commit(double* clocks, const int* collide, int n, cudaStream_t s);
 cudaError_t launch_collide_tri(const CollideArgs& a, cudaStream_t s, int cells_per_cta, int blocks);
 cudaError_t launch_nan_check(const double* f00, const void* planes, int planes_fp32, long long n_f00,
                              long long n_planes, const void* fields, long long n_fields, int* status,

@@ -1,0 +1,56 @@
+// Launcher of the pipelined RK4-stage kernel over a batch of independent
+// problems (the kernel is in stage_pipe.cuh): one persistent launch walks the
+// (problem, tile) list of every problem of the batch.
+#include "stage_pipe.cuh"
+
+namespace oshun {
+namespace {
+
+template <typename TS, int MC>
+cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaStream_t s) {
+    const SmemPlan P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes);
+    if (P.total > 227 * 1024) return cudaErrorNotSupported;
+    const int threads = nc + 64;
+    if (threads <= 256) return launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
+    if (threads <= 320) return launch_pipe<MC, TS, 320, true>(a1, bw, threads, P.total, bw.nitems, s);
+    return cudaErrorNotSupported;
+}
+
+}  // namespace
+
+size_t stage_batch_smem(const BatchWork& bw, int elem_bytes) {
+    return elem_bytes == 4 ? smem_plan<float>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes).total
+                           : smem_plan<double>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes).total;
+}
+
+void stage_batch_sizes(int np, int nx, int ny, int l0, int m0, int nc, int tx_cap, int elem_bytes, int* tx,
+                       size_t* slot_bytes, size_t* row_arr_bytes) {
+    *tx = tile_cells(np, nx, nc, tx_cap);
+    const PipeLayout L = pipe_layout((l0 + 1) * (m0 + 1), *tx, np, ny > 1, elem_bytes, m0);
+    *slot_bytes = L.slot_bytes;
+    *row_arr_bytes = L.row_arr_bytes;
+}
+
+int stage_batch_coef_bytes(int elem_bytes) {
+    return elem_bytes == 4 ? (int)sizeof(CoefT<float>) : (int)sizeof(CoefT<double>);
+}
+
+// nc consumer threads per CTA (a multiple of 32, <= 256); m0 of every problem <= mc
+template <typename TS>
+cudaError_t launch_stage_batch(const StageArgs<TS>& a1, const BatchWork& bw, int mc, int nc, cudaStream_t s) {
+    if (nc < 32 || nc > 256 || nc % 32) return cudaErrorInvalidValue;
+    switch (mc) {
+        case 0: return batch_mc<TS, 0>(a1, bw, nc, s);
+        case 1: return batch_mc<TS, 1>(a1, bw, nc, s);
+        case 2: return batch_mc<TS, 2>(a1, bw, nc, s);
+        case 3: return batch_mc<TS, 3>(a1, bw, nc, s);
+        case 4: return batch_mc<TS, 4>(a1, bw, nc, s);
+        case 6: return batch_mc<TS, 6>(a1, bw, nc, s);
+        case 8: return batch_mc<TS, 8>(a1, bw, nc, s);
+        default: return cudaErrorNotSupported;
+    }
+}
+template cudaError_t launch_stage_batch<double>(const StageArgs<double>&, const BatchWork&, int, int, cudaStream_t);
+template cudaError_t launch_stage_batch<float>(const StageArgs<float>&, const BatchWork&, int, int, cudaStream_t);
+
+}  // namespace oshun
