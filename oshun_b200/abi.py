@@ -86,6 +86,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_collide_flm_noalloc.argtypes = [ctypes.POINTER(OshunCfg), vp, vp, ctypes.c_double, vp,
                                               ctypes.POINTER(ctypes.c_longlong)]
     ip = ctypes.POINTER(ctypes.c_int)
+    if not hasattr(lib, "oshun_batch_create"):   # a build without the batch entry points
+        lib.oshun_last_error.restype = ctypes.c_char_p
+        lib.oshun_abi_version.restype = ctypes.c_int
+        _lib = lib
+        return lib
     lib.oshun_batch_create.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int, ip, ctypes.POINTER(vp)]
     lib.oshun_batch_destroy.argtypes = [vp]
     lib.oshun_batch_size.argtypes = [vp, ip]

@@ -1110,7 +1110,7 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
     b->mc = pick_mc(m0max);
     b->desc_bytes = (int)((std::max(sizeof(StageArgs<float>), sizeof(StageArgs<double>)) + 15) / 16 * 16);
     const int cbytes = stage_batch_coef_bytes(esz);
-    b->hdr_bytes = b->desc_bytes + cbytes * b->ncoef_max + (int)((sizeof(int) * b->ncoef_max + 15) / 16 * 16);
+    b->hdr_bytes = b->desc_bytes;
 
     // coupling tables in the arithmetic type
     std::vector<size_t> coff(n);
@@ -1165,8 +1165,11 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
     int pad_max = 32;
     for (oshun_ctx* h : b->P) pad_max = std::max(pad_max, ((h->cfg.nump + 31) / 32) * 32);
     b->nc = pad_max <= 192 ? 192 : 256;
-    b->tx_cap = 8;
-    int rc = batch_build_items(b);
+    int rc = OSHUN_ERR_UNSUPPORTED;
+    for (int tx : {8, 4, 2, 1}) {   // the widest tiles whose plan fits in shared memory
+        b->tx_cap = tx;
+        if ((rc = batch_build_items(b)) == OSHUN_OK) break;
+    }
     if (rc) return fail(rc);
     // device clocks and per-problem steps
     CKB(cudaMalloc(&b->d_clocks, sizeof(double) * 3 * n));

@@ -118,6 +118,25 @@ __device__ Smem carve(double* base, int np) {
     return s;
 }
 
+// e-e substeps and implicit step of one collision call: from the arguments,
+// or, when a device clock is given, by the reference's clock arithmetic for a
+// step ending at the clock's t (Explicit_EC_FP::loop, def-FokkerPlanck.cpp:
+// 598-599; Euler_Backward, :1277, 1297), as collide_params does on the host
+struct StepP {
+    int nsub;
+    double hsub, Dt;
+};
+__device__ __forceinline__ StepP step_params(const CollideArgs& a) {
+    StepP p{a.nsub, a.hsub, a.Dt};
+    if (a.clock) {
+        const double t = a.clock[0], t_ee = a.clock[1], t_eb = a.clock[2];
+        p.nsub = (int)((t - t_ee) / a.small_dt) + 1;
+        p.hsub = (t - t_ee) / (double)p.nsub;
+        p.Dt = t - t_eb;
+    }
+    return p;
+}
+
 // EE_isotropic_conserva::Getslope on warp 0: fh = C_ee(fin)
 __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin, double* fh) {
     const int n = a.np;
@@ -169,6 +188,7 @@ __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin,
 
 // Implicit_FLM_step::reset_coeff on warp 0 (f = f00 of the cell in smem)
 __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) {
+    const StepP sp = step_params(a);
     const int n = a.np;
     const int lane = threadIdx.x & 31;
     const double* vr = a.vr;
@@ -182,7 +202,7 @@ __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) 
     const double I0_density = I0[n - 1] * (4.0 * M_PI);
     const double lnee = log_ee(I0_density, I2_temperature, a.density_np);
     const double zlnei = zlog_ei(I0_density, I2_temperature, a.density_np, a.Zeta);
-    const double scale = (-1.0) * lnee * a.kpre * a.Dt;
+    const double scale = (-1.0) * lnee * a.kpre * sp.Dt;
     if (lane == 0) s.sc[0] = scale;
     for (int k = lane; k < n; k += 32) {
         double i2 = I2[k] * (4.0 * M_PI);
@@ -194,7 +214,7 @@ __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) 
         double sc = (k == 0) ? 0.0 : t1 * lnee;
         sc += zlnei * I0_density;
         sc /= a.U3[k];
-        sc *= a.kpre * a.Dt;
+        sc *= a.kpre * sp.Dt;
         s.scat[k] = sc;
         double ta = 0.0, tb = 0.0, tc = 0.0;
         if (k == 0) {
@@ -435,10 +455,11 @@ __device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell
 
 // e-e RK4 substeps of Explicit_EC_FP::loop on one warp (f00 of the cell in s.f)
 __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
+    const StepP sp = step_params(a);
     const int n = a.np;
     const int lane = threadIdx.x & 31;
-    for (int sub = 0; sub < a.nsub; ++sub) {
-        const double h = a.hsub;
+    for (int sub = 0; sub < sp.nsub; ++sub) {
+        const double h = sp.hsub;
         for (int k = lane; k < n; k += 32) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
         __syncwarp();
         ee_slope(a, s, s.f1, s.fh);
@@ -466,20 +487,7 @@ __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
     }
 }
 
-// the reference's clock arithmetic for one collision step ending at the
-// device clock's t (Explicit_EC_FP::loop, def-FokkerPlanck.cpp:598-599;
-// Euler_Backward, :1277, 1297), as collide_params does on the host
-__device__ __forceinline__ void apply_clock(CollideArgs& a) {
-    if (!a.clock) return;
-    const double t = a.clock[0], t_ee = a.clock[1], t_eb = a.clock[2];
-    a.nsub = (int)((t - t_ee) / a.small_dt) + 1;
-    a.hsub = (t - t_ee) / (double)a.nsub;
-    a.Dt = t - t_eb;
-}
-
-__global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideArgs a0) {
-    CollideArgs a = a0;
-    apply_clock(a);
+__global__ void __launch_bounds__(kCollideThreads) collide_kernel(const CollideArgs a) {
     extern __shared__ double smem[];
     const int n = a.np;
     Smem s = carve(smem, n);
@@ -525,9 +533,7 @@ __device__ __forceinline__ bool collided(const CollideArgs& a, int l, int m) {
 //      d'_i = (d_i - a_i d'_{i-1}) id_i (forward) and x_i = d'_i - c'_i x_{i+1}
 //      (backward); inside the run the lane applies the reference's recursion.
 template <typename TP>
-__global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a0) {
-    CollideArgs a = a0;
-    apply_clock(a);
+__global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
     extern __shared__ double smem[];
     const int n = a.np;
     const int l0 = a.l0;
@@ -849,10 +855,8 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
 }
 
 template <typename TP, int E, int P>
-__global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a0) {
+__global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
     extern __shared__ double smem[];
-    CollideArgs a = a0;
-    apply_clock(a);
     for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) collide_lane_cell<TP, E, P>(a, cell, smem);
 }
 
@@ -862,9 +866,7 @@ __global__ void __launch_bounds__(32) collide_lane_batch_kernel(const CollideBat
     extern __shared__ double smem[];
     for (long long it = blockIdx.x; it < b.nitems; it += gridDim.x) {
         const int2 w = b.items[it];
-        CollideArgs a = b.probs[w.x];
-        apply_clock(a);
-        collide_lane_cell<TP, E, P>(a, (long long)w.y, smem);
+        collide_lane_cell<TP, E, P>(b.probs[w.x], (long long)w.y, smem);
         __syncwarp();
     }
 }

@@ -107,8 +107,7 @@ cudaError_t launch_stage_fp64(const StageArgs<double>& a, int mc, cudaStream_t s
 // The work of one stage launch: a list of tiles, either of one problem (the
 // kernel parameter) or of a batch of problems (`probs` holds one StageArgs per
 // problem, `items` the (problem, tile) pairs).  In a batch the first bulk copy
-// of each tile also brings the problem's descriptor, its coupling table and
-// its plane map into the slot's header.
+// of each tile also brings the problem's descriptor into the slot's header.
 struct BatchWork {
     const unsigned char* probs;   // StageArgs<TS>[nprob], desc_bytes apart
     const int2* items;            // (problem, tile)
@@ -116,7 +115,7 @@ struct BatchWork {
     int tx_cap;                   // cells per tile at most
     int desc_bytes;               // sizeof(StageArgs<TS>) rounded to 16
     int ncoef_max;                // largest (l0+1)(m0+1) of the batch
-    int hdr_bytes;                // descriptor + coupling table + plane map
+    int hdr_bytes;                // slot header: the descriptor
     int slot_bytes, row_arr_bytes;   // largest slot / staged-row array of the batch
 };
 // batched stage kernel (stage_batch.cu); nc consumer threads per CTA

