@@ -45,7 +45,9 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="weibel2d")
+    ap.add_argument("--workload", default="weibel2d",
+                    help="weibel2d, weibel2d_64, landau1d, landau1d_large, relax1d, or batchN "
+                         "(N independent uneven 1D problems in one batch, e.g. batch512)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -243,8 +245,20 @@ def run_reference_arm(args, ws, rank):
     ncores = os.cpu_count() or 1
     vals, secs_all = [], []
     kind = sample = None
+    batch = args.workload.startswith("batch")
+    if batch:
+        from oshun_b200 import workloads
+        probs, _ = workloads.batch_problems(n=int(args.workload[len("batch"):] or 512), precision=0)
     for i in range(args.warmup + args.steps):
-        v, kind, sample, secs, used = cpu_sample_run(args.workload, ncores, steps=1)
+        if batch:
+            t0 = time.perf_counter()
+            r = cpu_batch_sample(probs, ncores)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference build (oracle/_ref) is missing"}))
+                return 0
+            v, kind, sample, secs, used = r[0], r[1], r[2], time.perf_counter() - t0, min(8, ncores)
+        else:
+            v, kind, sample, secs, used = cpu_sample_run(args.workload, ncores, steps=1)
         if i >= args.warmup:
             vals.append(v)
             secs_all.append(secs)
@@ -359,7 +373,131 @@ def run_ours(args, ws, rank, local):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms},
             "roofline": roofline,
-            "gpu_launches": 5 * args.steps,
+            # per step: 4 RK4 stage kernels, the clock advance, the collision kernel, the clock commit
+            "gpu_launches": 7 * args.steps,
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def batch_accounting(probs):
+    coefs = 0
+    step_bytes = 0
+    for cfg, _, _, col in probs:
+        a = accounting(cfg)
+        coefs += a["coef_updates"]
+        # RK4 16 words per element; the collision step 2 more when it runs
+        step_bytes += a["step_bytes"] if col else 4 * a["stage_bytes"]
+    return coefs, step_bytes
+
+
+def cpu_batch_sample(probs, nproc: int):
+    """The reference's own code on 8 sampled problems of the batch (those with
+    lmax >= 3, the reference's smallest supported case; 1D runs carry m <= 2
+    in the reference, only the batch's own harmonics are counted), one step
+    each, in parallel processes; returns (updates/s, kind, sample)."""
+    from oracle.cases import Deck, REF_BIN, State, reference_available, write_case  # checker only
+    from oshun_b200 import workloads
+    if not reference_available():
+        return None
+    pick = [i for i, (c, _, _, _) in enumerate(probs) if c["l0"] >= 3][:max(1, min(8, nproc))]
+    useful = 0
+    with tempfile.TemporaryDirectory() as td:
+        procs = []
+        for i in pick:
+            cfg, f, fields, col = probs[i]
+            d = Deck(l0=cfg["l0"], m0=2, nump=cfg["nump"], numx=cfg["numx"], numy=1, pmin=cfg["pmin"],
+                     pmax=cfg["pmax"], xmin=cfg["xmin"], xmax=cfg["xmax"], dt=cfg["dt"], small_dt=cfg["small_dt"],
+                     density_np=cfg["density_np"])
+            st = State(d)
+            for l in range(cfg["l0"] + 1):
+                st.f[d.ind(l, 0)] = f[l]
+            st.fields[:] = fields
+            fin = os.path.join(td, f"in{i}.case")
+            write_case(fin, st)
+            procs.append(subprocess.Popen([REF_BIN, fin, os.path.join(td, f"o{i}.case"),
+                                           f"step:1:{15 if col else 1}", "time"], stdout=subprocess.PIPE, text=True))
+            useful += workloads.num_harmonics(cfg["l0"], 0) * cfg["numx"] * cfg["nump"]
+        secs = max(float(p.communicate(timeout=900)[0].strip().split("elapsed_s=")[-1]) for p in procs)
+    return useful / secs, "reference", f"{len(pick)} problems of the batch with lmax >= 3, 1 step each, one process each"
+
+
+def run_batch(args, ws, rank, local):
+    """Batch of N independent uneven 1D problems (workloads.batch_problems),
+    FP32 bulk by default: one captured graph per step, tiles autotuned on the
+    batch itself before timing."""
+    import torch
+    from oshun_b200 import Batch, workloads
+    torch.cuda.set_device(local)
+    n = int(args.workload[len("batch"):] or 512)
+    prec = 0 if args.precision == "fp64" else 1
+    probs, meta = workloads.batch_problems(n=n, precision=prec, seed=2024 + rank)
+    coefs, step_bytes = batch_accounting(probs)
+    b = Batch([c for c, _, _, _ in probs], collide=[c for _, _, _, c in probs])
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    for i, (_, f, fl, _) in enumerate(probs):
+        b.upload(i, f, fl)
+    nc, tx, tune_ms = b.autotune(steps=2)
+    b.step(args.warmup)
+    torch.cuda.synchronize()
+    barrier(ws)
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms_total = reduce_max(e0.elapsed_time(e1), ws)
+    ms_step = ms_total / args.steps
+    value = coefs * args.steps * ws / (ms_total * 1e-3)
+    assert b.status() == 0
+    peak, peak_kind = measured_peaks()
+    achieved = step_bytes / (ms_step * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "kernel": "whole step (batched stage and collision kernels)",
+                "algorithmic_bytes_per_step": step_bytes}
+    # end to end: every step uploads every problem's state, steps, downloads it
+    ne = max(1, args.e2e_steps)
+    state_bytes = sum(int(f.nbytes + fl.nbytes) for _, f, fl, _ in probs)
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(ne):
+        for i, (_, f, fl, _) in enumerate(probs):
+            b.upload(i, f, fl)
+        b.step(1)
+        for i in range(n):
+            b.download(i)
+    q1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(q0.elapsed_time(q1), ws) / ne
+    b.close()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        r = cpu_batch_sample(probs, os.cpu_count() or 1)
+        if r:
+            cpu = {"value": r[0], "unit": UNIT, "cores": min(8, os.cpu_count() or 1), "kind": r[1], "sample": r[2]}
+    if rank == 0:
+        nsteps_groups = 4 + 2 + len({(c["nump"] + 31) // 32 for c, _, _, col in probs if col})
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32+f64", "data": "synthetic",
+            "config": {"workload": args.workload, "precision": args.precision, "problems": n,
+                       "coefficients": coefs, "seed": meta["seed"], "stage_threads": nc, "tile_cells": tx,
+                       "autotune_ms_per_step": round(tune_ms, 4),
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                       "l2": "inputs larger than L2"},
+            "e2e": {"value": coefs * ws / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms},
+            "roofline": roofline,
+            "gpu_launches": nsteps_groups * args.steps,
             "clocks": clocks,
         }
         if cpu is not None:
@@ -376,6 +514,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference_arm(args, ws, rank)
+        if args.workload.startswith("batch"):
+            return run_batch(args, ws, rank, local)
         return run_ours(args, ws, rank, local)
     finally:
         if ws > 1:

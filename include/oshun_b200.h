@@ -158,6 +158,9 @@ int oshun_plane_index(oshun_handle h, int l, int m, int* plane);
 typedef struct oshun_batch_ctx* oshun_batch;
 int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_batch* out);
 int oshun_batch_destroy(oshun_batch b);
+/* Runs the batch's work on this cudaStream_t (NULL = the batch's own stream);
+ * the captured graphs are rebuilt on the next step. */
+int oshun_batch_set_stream(oshun_batch b, void* stream);
 int oshun_batch_size(oshun_batch b, int* n);
 /* the handle of problem i (owned by the batch; its queries and transfers work,
  * its stream is the batch's) */

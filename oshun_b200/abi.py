@@ -27,7 +27,7 @@ EXPORTED = [
     "oshun_download", "oshun_rhs", "oshun_rk4_step", "oshun_collide_ee", "oshun_collide_f1",
     "oshun_collide_flm", "oshun_step", "oshun_time", "oshun_status_flags", "oshun_device_state",
     "oshun_plane_index", "oshun_last_error", "oshun_abi_version", "oshun_collide_flm_noalloc",
-    "oshun_batch_create", "oshun_batch_destroy", "oshun_batch_size", "oshun_batch_problem",
+    "oshun_batch_create", "oshun_batch_destroy", "oshun_batch_set_stream", "oshun_batch_size", "oshun_batch_problem",
     "oshun_batch_upload", "oshun_batch_download", "oshun_batch_step", "oshun_batch_status",
     "oshun_batch_set_tiles", "oshun_batch_get_tiles", "oshun_batch_autotune",
 ]
@@ -94,6 +94,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_batch_create.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int, ip, ctypes.POINTER(vp)]
     lib.oshun_batch_destroy.argtypes = [vp]
     lib.oshun_batch_size.argtypes = [vp, ip]
+    lib.oshun_batch_set_stream.argtypes = [vp, vp]
     lib.oshun_batch_problem.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
     lib.oshun_batch_upload.argtypes = [vp, ctypes.c_int, vp, vp]
     lib.oshun_batch_download.argtypes = [vp, ctypes.c_int, vp, vp]
@@ -281,6 +282,11 @@ class Batch:
 
     def step(self, nsteps: int = 1) -> None:
         self._check(self.lib.oshun_batch_step(self._b, nsteps), "oshun_batch_step")
+
+    def set_stream(self, stream_ptr: int) -> None:
+        """Run on this cudaStream_t (an integer handle, 0 = the batch's own stream)."""
+        self._check(self.lib.oshun_batch_set_stream(self._b, ctypes.c_void_p(stream_ptr or None)),
+                    "oshun_batch_set_stream")
 
     def status(self) -> int:
         f = ctypes.c_int()

@@ -903,6 +903,7 @@ struct oshun_batch_ctx {
     int2* d_items = nullptr;
     int nitems = 0;
     size_t slot_bytes = 0, row_arr_bytes = 0;
+    int row_depth = 2;
     std::vector<unsigned char> h_a1[2][4];   // kernel parameter of each launch (a problem's descriptor)
     // collision launches
     struct Group {
@@ -980,8 +981,11 @@ int batch_build_items(oshun_batch_ctx* b) {
         const double cost = (double)b->P[i]->nh * (double)(((c.nump + 31) / 32) * 32) * tx;
         for (int t = 0; t < tiles; ++t) items.push_back({cost, i, t});
     }
+    // staged-row ring: as deep as 24 KB of rows allow, 2..8 rows
+    b->row_depth = (int)std::max<size_t>(2, std::min<size_t>(8, (24 * 1024) / std::max<size_t>(1, 2 * rowb)));
     BatchWork bw{};
     bw.hdr_bytes = b->hdr_bytes; bw.slot_bytes = (int)slot; bw.row_arr_bytes = (int)rowb;
+    bw.row_depth = b->row_depth;
     if (stage_batch_smem(bw, esz) > 227 * 1024) {
         set_error("batch tiles do not fit in shared memory (lower the cells per tile)");
         return OSHUN_ERR_UNSUPPORTED;
@@ -1010,6 +1014,7 @@ BatchWork batch_work(const oshun_batch_ctx* b, int c, int k) {
     bw.hdr_bytes = b->hdr_bytes;
     bw.slot_bytes = (int)b->slot_bytes;
     bw.row_arr_bytes = (int)b->row_arr_bytes;
+    bw.row_depth = b->row_depth;
     return bw;
 }
 
@@ -1224,6 +1229,24 @@ int oshun_batch_destroy(oshun_batch b) {
     if (!b) return OSHUN_ERR_ARG;
     cudaStreamSynchronize(b->stream);
     free_batch(b);
+    return OSHUN_OK;
+}
+
+int oshun_batch_set_stream(oshun_batch b, void* stream) {
+    if (!b) return OSHUN_ERR_ARG;
+    CK(cudaStreamSynchronize(b->stream));
+    batch_drop_graphs(b);
+    b->graphs_ok = true;
+    cudaStream_t next = (cudaStream_t)stream;
+    if (!next) CK(cudaStreamCreateWithFlags(&next, cudaStreamNonBlocking));
+    // the problems move first: oshun_set_stream waits on their current (the old) stream
+    for (oshun_ctx* h : b->P) {
+        int rc = oshun_set_stream(h, next);
+        if (rc) return rc;
+    }
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    b->stream = next;
+    b->own_stream = stream == nullptr;
     return OSHUN_OK;
 }
 

@@ -117,6 +117,7 @@ struct BatchWork {
     int ncoef_max;                // largest (l0+1)(m0+1) of the batch
     int hdr_bytes;                // slot header: the descriptor
     int slot_bytes, row_arr_bytes;   // largest slot / staged-row array of the batch
+    int row_depth;                // staged-row ring depth (2..8)
 };
 // batched stage kernel (stage_batch.cu); nc consumer threads per CTA
 template <typename TS>

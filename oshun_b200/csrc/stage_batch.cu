@@ -8,7 +8,7 @@ namespace {
 
 template <typename TS, int MC>
 cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaStream_t s) {
-    const SmemPlan P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes);
+    const SmemPlan P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth);
     if (P.total > 227 * 1024) return cudaErrorNotSupported;
     const int threads = nc + 64;
     if (threads <= 256) return launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
@@ -19,8 +19,8 @@ cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaS
 }  // namespace
 
 size_t stage_batch_smem(const BatchWork& bw, int elem_bytes) {
-    return elem_bytes == 4 ? smem_plan<float>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes).total
-                           : smem_plan<double>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes).total;
+    return elem_bytes == 4 ? smem_plan<float>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth).total
+                           : smem_plan<double>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth).total;
 }
 
 void stage_batch_sizes(int np, int nx, int ny, int l0, int m0, int nc, int tx_cap, int elem_bytes, int* tx,

@@ -359,12 +359,14 @@ __host__ __device__ inline int tile_cells(int np, int nx, int nc, int tx_cap) {
 struct SmemPlan {
     size_t off_cur, off_coef, off_plane, off_sj, off_slots, slot_stride, hdr, off_rows, row_arr_bytes, total;
 };
+// barriers at offset 0: full[kDepth], empty[kDepth], rowfull[kRowMax], rowempty[kRowMax]
+constexpr int kRowMax = 8;
 template <typename TS>
 __host__ __device__ inline SmemPlan smem_plan(bool batch, int hdr_bytes, int ncoef, size_t slot_bytes,
-                                              size_t row_arr_bytes) {
+                                              size_t row_arr_bytes, int row_depth = 2) {
     SmemPlan P;
     P.hdr = batch ? (size_t)hdr_bytes : 0;
-    P.off_cur = 256;                                   // batch: current item's header, two buffers
+    P.off_cur = 512;                                   // batch: current item's header, two buffers
     P.off_coef = P.off_cur + 2 * P.hdr;                // single problem: coupling table, plane map
     P.off_plane = align_up(P.off_coef + (batch ? 0 : sizeof(CoefT<TS>) * (size_t)ncoef), 16);
     P.off_sj = align_up(P.off_plane + (batch ? 0 : sizeof(int) * (size_t)ncoef), 16);
@@ -372,12 +374,19 @@ __host__ __device__ inline SmemPlan smem_plan(bool batch, int hdr_bytes, int nco
     P.slot_stride = align_up(P.hdr + slot_bytes, 128);
     P.off_rows = P.off_slots + kDepth * P.slot_stride;
     P.row_arr_bytes = row_arr_bytes;
-    P.total = P.off_rows + 2 * 2 * row_arr_bytes;      // [buffer][B, A]
+    P.total = P.off_rows + (size_t)row_depth * 2 * row_arr_bytes;   // [buffer][B, A]
     return P;
 }
 
+// resident CTAs per SM the batched kernel is compiled for: two when the
+// accumulators are few (m0 <= 1, the 1D batches), so that one CTA's tile
+// start and end latencies overlap the other's work
+template <int MC, bool BATCH>
+constexpr int batch_min_blocks() { return (BATCH && MC <= 1) ? 2 : 1; }
+
 template <int MC, typename TS, int MAXT, bool BATCH>
-__global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<TS> a1, const BatchWork bw) {
+__global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, BATCH>())
+    rk_stage_pipe_kernel(const StageArgs<TS> a1, const BatchWork bw) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;
     const int nc = (int)blockDim.x - 64;               // consumer threads
@@ -385,7 +394,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
     SmemPlan P;
     int ntiles1 = 0;
     if constexpr (BATCH) {
-        P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes);
+        P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth);
     } else {
         const int ncoef = (a1.l0 + 1) * (a1.m0 + 1);
         const int tx = tile_cells(a1.np, a1.nx, nc, bw.tx_cap);
@@ -397,7 +406,9 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + kDepth;
     uint64_t* rowfull = empty + kDepth;
-    uint64_t* rowempty = rowfull + 2;
+    uint64_t* rowempty = rowfull + kRowMax;
+    // staged-row ring depth: a batch of few harmonics per row needs rows further ahead
+    const int RD = BATCH ? bw.row_depth : 2;
     double* sj = reinterpret_cast<double*>(smem + P.off_sj);   // [2 items][3][8 cells][8 warps]
     unsigned char* slots = smem + P.off_slots;
     unsigned char* rows = smem + P.off_rows;
@@ -413,7 +424,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
     }
     if (tid == 0) {
         for (int k = 0; k < kDepth; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
-        for (int k = 0; k < 2; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
+        for (int k = 0; k < RD; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -506,12 +517,12 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
                     }
                 }
             } else {
-                // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
+                // row warp: Y0 (and Y) of each target row, up to RD rows ahead of its epilogue
                 const bool need_A = !a.first;
                 const long long base_cell = row + x0;
                 long long q0 = 0;   // first plane of row t (planes in (l, m) order)
                 for (int t = 0; t <= a.l0; ++t) {
-                    const int rb = issued & 1, k = issued >> 1;
+                    const int rb = issued % RD, k = issued / RD;
                     if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1))) { ok = false; break; }
                     unsigned char* base = rows + (size_t)rb * 2 * P.row_arr_bytes;
                     const uint32_t nb = need_A ? 2 : 1;
@@ -543,8 +554,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
                 for (int idx = max(0, issued - kDepth); idx < issued; ++idx)
                     mbar_wait(full + (idx % kDepth), (uint32_t)((idx / kDepth) & 1));
             } else {
-                for (int t = max(0, issued - 2); t < issued; ++t)
-                    mbar_wait(rowfull + (t & 1), (uint32_t)((t >> 1) & 1));
+                for (int t = max(0, issued - RD); t < issued; ++t)
+                    mbar_wait(rowfull + (t % RD), (uint32_t)((t / RD) & 1));
             }
         }
         return;
@@ -637,8 +648,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_pipe_kernel(const StageArgs<
 
         // RK epilogue of target row t from the staged Y0/Y rows
         auto epilogue = [&](const int t) {
-            const int rb = rows_used & 1;
-            if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
+            const int rb = rows_used % RD;
+            if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used / RD) & 1))) {
                 atomicOr(err, 16);
                 dead = true;
                 }
@@ -780,8 +791,16 @@ cudaError_t launch_pipe(const StageArgs<TS>& a, const BatchWork& bw, int threads
         if (e != cudaSuccess) return e;
         attr = smem;
     }
-    // one resident CTA per SM, each walking items blockIdx.x + k gridDim.x
-    const long long blocks = nitems < sm_count() ? nitems : sm_count();
+    // persistent CTAs, as many as are resident at once, each walking items
+    // blockIdx.x + k gridDim.x
+    int per_sm = 1;
+    if (BATCH) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rk_stage_pipe_kernel<MC, TS, MAXT, BATCH>,
+                                                                      threads, smem);
+        if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    }
+    const long long cap = (long long)per_sm * sm_count();
+    const long long blocks = nitems < cap ? nitems : cap;
     if (blocks < 1) return cudaSuccess;
     rk_stage_pipe_kernel<MC, TS, MAXT, BATCH><<<dim3((unsigned)blocks), dim3(threads), smem, s>>>(a, bw);
     return cudaGetLastError();

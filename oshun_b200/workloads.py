@@ -187,8 +187,9 @@ def batch_problems(n: int = 512, seed: int = 2024, precision: int = 1, vth: floa
         dt = min(0.05, 0.5 * dx / vmax)
         pmin = pmax / (2.0 * nump)
         density = density_for_nu(nu, vth) if nu > 0 else 1e21
+        # small_dt above dt: one e-e substep per step (the reference takes floor(dt/small_dt) + 1)
         cfg = _base_cfg(l0=l0, m0=0, nump=nump, numx=nx, numy=1, pmin=pmin, pmax=pmax, xmin=0.0,
-                        xmax=L * (nx - 1) / nx, dt=dt, small_dt=dt, density_np=density, precision=precision)
+                        xmax=L * (nx - 1) / nx, dt=dt, small_dt=1.5 * dt, density_np=density, precision=precision)
         p = p_axis(nump, pmin, pmax)
         x = np.arange(nx) * dx
         dens = 1.0 + 1e-3 * np.cos(k * x + phase)

@@ -51,9 +51,11 @@ def _solo(cfg, st, nsteps, collide):
         return h.download()
 
 
-def _batch(problems, nsteps, collide, tiles=None, autotune=False):
+def _batch(problems, nsteps, collide, tiles=None, autotune=False, stream=None):
     from oshun_b200 import Batch
     with Batch([c for c, _ in problems], collide=collide) as b:
+        if stream is not None:
+            b.set_stream(stream.cuda_stream)
         for i, (_, st) in enumerate(problems):
             b.upload(i, st.f, st.fields)
         if autotune:
@@ -80,6 +82,17 @@ def test_batch_matches_solo_runs(precision, tiles):
         fs, fls = _solo(cfg, st, 4, col)
         assert np.array_equal(f, fs), cfg
         assert np.array_equal(fl, fls), cfg
+
+
+def test_batch_on_a_caller_stream():
+    import torch
+    problems = _mixed(0)
+    collide = [True] * len(problems)
+    stream = torch.cuda.Stream()
+    got = _batch(problems, 3, collide, stream=stream)
+    for (cfg, st), (f, fl) in zip(problems, got):
+        fs, fls = _solo(cfg, st, 3, True)
+        assert np.array_equal(f, fs) and np.array_equal(fl, fls)
 
 
 def test_batch_rejects_narrow_tiles():
