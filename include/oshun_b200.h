@@ -180,6 +180,31 @@ int oshun_batch_get_tiles(oshun_batch b, int* stage_threads, int* tile_cells);
  * and restores the state and clocks; returns the choice and its ms/step. */
 int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile_cells, double* ms_per_step);
 
+/* ---- adjoint of the small step ------------------------------------------- */
+
+/* No counterpart in the reference, which computes no derivatives.  For 1D
+ * runs with m0 = 0 (numy = 1, FP64, tridiagonal collisions, nump <= 256):
+ * the vector-Jacobian product of one small step (oshun_step's sequence:
+ * RK4 Vlasov-Maxwell step, then, with `collisions`, the e-e substeps and the
+ * implicit f_l solves).  State vectors are device arrays of
+ * oshun_adjoint_state_size doubles in the plane layout: the f00 plane, the
+ * l >= 1 planes (f[l][x][p]), the 6 field planes.  (t, t_ee, t_eb) are the
+ * RK, e-e and implicit clocks before the step (Runge_Kutta_4::t,
+ * Explicit_EC_FP::t, Euler_Backward::t): they fix the step's e-e substeps
+ * and implicit step as in the forward.  Cotangents of the fields other than
+ * E_x come back zero: with m0 = 0 they never act on f or E_x. */
+typedef struct oshun_adj_ctx* oshun_adjoint;
+int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out);
+int oshun_adjoint_destroy(oshun_adjoint a);
+int oshun_adjoint_set_stream(oshun_adjoint a, void* stream);
+int oshun_adjoint_state_size(oshun_adjoint a, long long* n);
+/* y_next = step(y) through the production kernels */
+int oshun_adjoint_forward(oshun_adjoint a, const double* y, double* y_next, int collisions, double t, double t_ee,
+                          double t_eb);
+/* lam = (d step / d y)^T lam_next at y (stage states recomputed from y) */
+int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, double* lam, int collisions, double t,
+                      double t_ee, double t_eb);
+
 /* ---- allocation-free collision step --------------------------------------- */
 
 /* No counterpart in the reference.  The implicit f_lm collision step (the work

@@ -30,6 +30,8 @@ EXPORTED = [
     "oshun_batch_create", "oshun_batch_destroy", "oshun_batch_set_stream", "oshun_batch_size", "oshun_batch_problem",
     "oshun_batch_upload", "oshun_batch_download", "oshun_batch_step", "oshun_batch_status",
     "oshun_batch_set_tiles", "oshun_batch_get_tiles", "oshun_batch_autotune",
+    "oshun_adjoint_create", "oshun_adjoint_destroy", "oshun_adjoint_set_stream", "oshun_adjoint_state_size",
+    "oshun_adjoint_forward", "oshun_adjoint_vjp",
 ]
 
 
@@ -103,6 +105,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_batch_set_tiles.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.oshun_batch_get_tiles.argtypes = [vp, ip, ip]
     lib.oshun_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ip, dp]
+    if hasattr(lib, "oshun_adjoint_create"):
+        d = ctypes.c_double
+        lib.oshun_adjoint_create.argtypes = [ctypes.POINTER(OshunCfg), ctypes.POINTER(vp)]
+        lib.oshun_adjoint_destroy.argtypes = [vp]
+        lib.oshun_adjoint_set_stream.argtypes = [vp, vp]
+        lib.oshun_adjoint_state_size.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+        lib.oshun_adjoint_forward.argtypes = [vp, vp, vp, ctypes.c_int, d, d, d]
+        lib.oshun_adjoint_vjp.argtypes = [vp, vp, vp, vp, ctypes.c_int, d, d, d]
     lib.oshun_last_error.restype = ctypes.c_char_p
     lib.oshun_abi_version.restype = ctypes.c_int
     _lib = lib

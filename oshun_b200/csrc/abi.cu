@@ -1429,3 +1429,202 @@ int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of the small step, 1D with m0 = 0, FP64 (no counterpart in the
+// reference, which has no derivatives).  oshun_adjoint_forward runs one step
+// of the production path on caller-owned device vectors; oshun_adjoint_vjp
+// recomputes that step's RK4 stage states with the production stage kernels
+// and applies the transposes of adjoint.cu:
+//   lambda_1 = cotangent of the step's output;
+//   collision step transpose (if collisions) at the RK4 output y1;
+//   RK4 transpose, s1..s4 the stage inputs, h the step:
+//     a4 = F'(s4)^T (h/6 l), a3 = F'(s3)^T (h/3 l + h a4),
+//     a2 = F'(s2)^T (h/3 l + h/2 a3), a1 = F'(s1)^T (h/6 l + h/2 a2),
+//     lambda_0 = l + a1 + a2 + a3 + a4.
+// ---------------------------------------------------------------------------
+struct oshun_adj_ctx {
+    oshun_ctx* h = nullptr;
+    long long n = 0;                 // doubles of one state vector
+    double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *y1 = nullptr;
+    double *lam1 = nullptr, *c = nullptr, *a = nullptr, *acc = nullptr;
+    adj::Coef1* d_coef1 = nullptr;
+    double* ws = nullptr;
+    long long ws_cap = 0;            // doubles
+};
+
+namespace {
+
+int adj_copy_in(oshun_ctx* h, int set, const double* y) {
+    const size_t pb = sizeof(double) * h->pstride;
+    CK(cudaMemcpyAsync(h->f00[set], y, pb, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->pl[set], y + h->pstride, pb * h->nplanes, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->fld[set], y + (1 + (long long)h->nplanes) * h->pstride, sizeof(double) * 6 * h->cells,
+                       cudaMemcpyDeviceToDevice, h->stream));
+    return OSHUN_OK;
+}
+int adj_copy_out(oshun_ctx* h, int set, double* y) {
+    const size_t pb = sizeof(double) * h->pstride;
+    CK(cudaMemcpyAsync(y, h->f00[set], pb, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(y + h->pstride, h->pl[set], pb * h->nplanes, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(y + (1 + (long long)h->nplanes) * h->pstride, h->fld[set], sizeof(double) * 6 * h->cells,
+                       cudaMemcpyDeviceToDevice, h->stream));
+    return OSHUN_OK;
+}
+
+void free_adj(oshun_adj_ctx* a) {
+    if (a->h) free_ctx(a->h);
+    cudaFree(a->s2); cudaFree(a->s3); cudaFree(a->s4); cudaFree(a->y1);
+    cudaFree(a->lam1); cudaFree(a->c); cudaFree(a->a); cudaFree(a->acc);
+    cudaFree(a->d_coef1); cudaFree(a->ws);
+    delete a;
+}
+
+adj::Grid1 adj_grid(const oshun_adj_ctx* a) {
+    const oshun_ctx* h = a->h;
+    adj::Grid1 g;
+    g.np = h->cfg.nump; g.nx = h->cfg.numx; g.l0 = h->cfg.l0;
+    g.invp = h->d_ptab; g.vr = h->d_ptab + h->cfg.nump; g.wj = h->d_ptab + 2 * h->cfg.nump;
+    g.coef = a->d_coef1;
+    g.g00_s = h->g00_s; g.g00_inv = h->g00_inv; g.g00_gr = h->g00_gr;
+    return g;
+}
+
+adj::CollTables adj_tables(const oshun_ctx* h) {
+    adj::CollTables T;
+    const int np = h->cfg.nump;
+    const double* V = h->d_vtab;
+    T.np = np; T.NB = h->cfg.NB_algorithms;
+    T.vr = V; T.U4 = V + np; T.U4m1 = V + 2 * np; T.U2 = V + 3 * np; T.U2m1 = V + 4 * np;
+    T.U1 = V + 5 * np; T.U1m1 = V + 6 * np; T.U3 = V + 7 * np; T.Qn = V + 8 * np; T.Pn = V + 9 * np;
+    T.V5 = V + 10 * np; T.V7 = V + 11 * np;
+    T.density_np = h->cfg.density_np; T.Zeta = h->cfg.Zeta; T.c_kpre = h->c_kpre; T.kpre = h->kpre;
+    return T;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out) {
+    if (!out || !cfg) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    *out = nullptr;
+    if (cfg->numy != 1 || cfg->m0 != 0 || cfg->precision != OSHUN_FP64 || !cfg->if_tridiagonal ||
+        ((cfg->nump + 31) / 32) * 32 > 256) {
+        set_error("the adjoint covers 1D runs (numy = 1) with m0 = 0, FP64, tridiagonal collisions, nump <= 256");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
+    oshun_adj_ctx* a = new oshun_adj_ctx();
+    int rc = oshun_create(cfg, &a->h);
+    if (rc) { delete a; return rc; }
+    oshun_ctx* h = a->h;
+    a->n = (1 + (long long)h->nplanes) * h->pstride + 6 * h->cells;
+    auto fail = [&](int code) { free_adj(a); return code; };
+    double** bufs[] = {&a->s2, &a->s3, &a->s4, &a->y1, &a->lam1, &a->c, &a->a, &a->acc};
+    for (double** b : bufs)
+        if (cudaMalloc(b, sizeof(double) * a->n) != cudaSuccess) { set_error("cudaMalloc failed"); return fail(OSHUN_ERR_CUDA); }
+    const int l0 = cfg->l0;
+    std::vector<double> cf((size_t)(l0 + 1) * 16);
+    std::vector<adj::Coef1> c1(l0 + 1);
+    if (cudaMemcpy(cf.data(), h->d_coef, sizeof(double) * cf.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error("coefficient copy failed");
+        return fail(OSHUN_ERR_CUDA);
+    }
+    for (int l = 0; l <= l0; ++l) {
+        const CoefLM* k = reinterpret_cast<const CoefLM*>(cf.data()) + l;
+        c1[l] = adj::Coef1{k->ex_g, k->ex_h, k->ax_p, k->ax_m, k->gfac, k->invpax, k->hp0};
+    }
+    if (cudaMalloc(&a->d_coef1, sizeof(adj::Coef1) * c1.size()) != cudaSuccess ||
+        cudaMemcpy(a->d_coef1, c1.data(), sizeof(adj::Coef1) * c1.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        set_error("coefficient upload failed");
+        return fail(OSHUN_ERR_CUDA);
+    }
+    *out = a;
+    return OSHUN_OK;
+}
+
+int oshun_adjoint_destroy(oshun_adjoint a) {
+    if (!a) return OSHUN_ERR_ARG;
+    cudaStreamSynchronize(a->h->stream);
+    free_adj(a);
+    return OSHUN_OK;
+}
+
+int oshun_adjoint_set_stream(oshun_adjoint a, void* stream) {
+    if (!a) return OSHUN_ERR_ARG;
+    return oshun_set_stream(a->h, stream);
+}
+
+int oshun_adjoint_state_size(oshun_adjoint a, long long* n) {
+    if (!a || !n) return OSHUN_ERR_ARG;
+    *n = a->n;
+    return OSHUN_OK;
+}
+
+int oshun_adjoint_forward(oshun_adjoint a, const double* y, double* y_next, int collisions, double t, double t_ee,
+                          double t_eb) {
+    if (!a || !y || !y_next) return OSHUN_ERR_ARG;
+    oshun_ctx* h = a->h;
+    int rc = adj_copy_in(h, h->cur, y);
+    if (rc) return rc;
+    h->t = t; h->t_ee = t_ee; h->t_eb = t_eb;
+    if ((rc = oshun_step(h, 1, collisions))) return rc;
+    if ((rc = adj_copy_out(h, h->cur, y_next))) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, double* lam, int collisions, double t,
+                      double t_ee, double t_eb) {
+    if (!a || !y || !lam_next || !lam) return OSHUN_ERR_ARG;
+    oshun_ctx* h = a->h;
+    const double dt = h->cfg.dt;
+    const int B = h->cur, A = h->cur ^ 1, Sa = 2, Sb = 3;
+    int rc;
+    // stage inputs of the step (the production stage kernels)
+    if ((rc = adj_copy_in(h, B, y))) return rc;
+    if ((rc = launch_stage(h, B, B, A, Sa, 0, 1, 0.5 * dt, 1.0 / 3.0))) return rc;
+    if ((rc = adj_copy_out(h, Sa, a->s2))) return rc;
+    if ((rc = launch_stage(h, Sa, B, A, Sb, 0, 0, 0.5 * dt, 2.0 / 3.0))) return rc;
+    if ((rc = adj_copy_out(h, Sb, a->s3))) return rc;
+    if ((rc = launch_stage(h, Sb, B, A, Sa, 0, 0, dt, 1.0 / 3.0))) return rc;
+    if ((rc = adj_copy_out(h, Sa, a->s4))) return rc;
+    if ((rc = launch_stage(h, Sa, B, A, -1, 0, 0, dt / 6.0, 1.0))) return rc;
+    if ((rc = adj_copy_out(h, A, a->y1))) return rc;
+    CK(cudaMemcpyAsync(a->lam1, lam_next, sizeof(double) * a->n, cudaMemcpyDeviceToDevice, h->stream));
+    // collision step transpose at y1
+    if (collisions) {
+        const double t_new = t + dt;
+        const int nsub = (int)((t_new - t_ee) / h->cfg.small_dt) + 1;   // def-FokkerPlanck.cpp:598-599
+        const double hsub = (t_new - t_ee) / (double)nsub;
+        const double Dt = t_new - t_eb;
+        const long long wsz = adj::coll_ws(h->cfg.nump, h->cfg.l0, nsub);
+        if (wsz * h->cfg.numx > a->ws_cap) {
+            CK(cudaStreamSynchronize(h->stream));
+            cudaFree(a->ws);
+            a->ws = nullptr;
+            CK(cudaMalloc(&a->ws, sizeof(double) * wsz * h->cfg.numx));
+            a->ws_cap = wsz * h->cfg.numx;
+        }
+        CK(launch_collide_adj(adj_tables(h), h->cfg.l0, h->cfg.numx, a->y1, a->lam1, 1, 1, nsub, hsub, Dt, a->ws, wsz,
+                              h->stream));
+    }
+    // RK4 transpose
+    const adj::Grid1 g = adj_grid(a);
+    const long long n = a->n;
+    CK(cudaMemcpyAsync(a->acc, a->lam1, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    const double* S[4] = {y, a->s2, a->s3, a->s4};
+    const double w_out[4] = {dt / 6.0, dt / 3.0, dt / 3.0, dt / 6.0};
+    const double w_in[4] = {0.0, 0.5 * dt, 0.5 * dt, dt};   // weight of k_{i-1} in s_i
+    for (int st = 3; st >= 0; --st) {
+        if (st == 3) CK(launch_rk_combine(a->c, a->lam1, w_out[3], a->lam1, 0.0, nullptr, 0.0, n, h->stream));
+        else CK(launch_rk_combine(a->c, a->lam1, w_out[st], a->a, w_in[st + 1], nullptr, 0.0, n, h->stream));
+        CK(launch_stage_vjp(g, S[st], a->c, a->a, h->stream));
+        CK(launch_rk_combine(a->acc, a->acc, 1.0, a->a, 1.0, nullptr, 0.0, n, h->stream));
+    }
+    CK(cudaMemcpyAsync(lam, a->acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+}  // extern "C"

@@ -1,6 +1,7 @@
 // Internal declarations shared by the CUDA translation units of liboshun_b200.
 #pragma once
 
+#include "adjoint_math.h"
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -132,6 +133,12 @@ size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal);
 int collide_max_chunk(int np, size_t smem_budget);
 int collide_threads();
 size_t collide_tri_smem_per_cell(int np, int l0);
+// adjoint kernels of the 1D m0 = 0 step (adjoint.cu; types in adjoint_math.h)
+cudaError_t launch_stage_vjp(const adj::Grid1& g, const double* s, const double* c, double* out, cudaStream_t st);
+cudaError_t launch_collide_adj(const adj::CollTables& T, int l0, int nx, const double* y, double* lam, int ee, int eb,
+                               int nsub, double hsub, double Dt, double* ws, long long wsz, cudaStream_t st);
+cudaError_t launch_rk_combine(double* out, const double* v0, double a0, const double* v1, double a1, const double* v2,
+                              double a2, long long n, cudaStream_t st);
 // tridiagonal collision step of a batch whose problems share E = ceil(np/32) <= 8
 cudaError_t launch_collide_batch(const CollideBatch& b, int E, int planes_fp32, size_t smem, cudaStream_t s);
 // device clocks {t, t_ee, t_eb} of n problems: t += dt; after a collision step t_ee = t_eb = t

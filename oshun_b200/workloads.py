@@ -203,6 +203,45 @@ def batch_problems(n: int = 512, seed: int = 2024, precision: int = 1, vth: floa
     return out, meta
 
 
+def sensitivity1d(nx: int = 512, l0: int = 2, nump: int = 128, vth: float = 0.05, seed: int = 11,
+                  nu_dt: float = 0.05, dt: float = 0.5, length: float = 100.0, ee_substeps: int = 5):
+    """Sensitivity configuration: 1D periodic, nx = 512 cells over `length`
+    (c/w_p), lmax = 2, np = 128 to 8 v_th, uniform density, T(x) = T0 (1 + 0.2
+    g(x)) with g a seeded smooth random field of 8 Fourier modes (max |g| =
+    1), nu_ei dt = 0.05 (the density that gives that nu at v_th), dt = 0.5/w_p
+    (explicit advection stable: v_max dt/dx < 1), small_dt = dt/5 (the
+    explicit e-e step stable).  Returns cfg, the relative temperature tau(x) =
+    T/T0, meta."""
+    nu = nu_dt / dt
+    pmax = 8.0 * vth
+    pmin = pmax / (2.0 * nump)
+    cfg = _base_cfg(l0=l0, m0=0, nump=nump, numx=nx, numy=1, pmin=pmin, pmax=pmax, xmin=0.0,
+                    xmax=length * (nx - 1) / nx, dt=dt, small_dt=dt / ee_substeps,
+                    density_np=density_for_nu(nu, vth), precision=0)
+    rng = np.random.default_rng(seed)
+    x = np.arange(nx) * (length / nx)
+    g = np.zeros(nx)
+    for k in range(1, 9):
+        g += rng.standard_normal() / k * np.cos(2.0 * np.pi * k * x / length + rng.uniform(0, 2 * np.pi))
+    g /= np.max(np.abs(g))
+    tau = 1.0 + 0.2 * g
+    meta = dict(workload="sensitivity1d", nx=nx, lmax=l0, np=nump, nu_ei=nu, vth=vth, seed=seed)
+    return cfg, tau, meta
+
+
+def sensitivity_state(cfg: dict, tau, vth: float = 0.05):
+    """plane-layout FP64 state (torch, on tau's device) of a Maxwellian of
+    temperature vth^2 tau(x) per cell (Setup_Y::Gaussian_p, OSHUN-1/
+    def-Setup.cpp:500-533), f_l = 0 for l >= 1, no fields; differentiable in tau"""
+    import torch
+    nx, np_, l0 = cfg["numx"], cfg["nump"], cfg["l0"]
+    p = torch.tensor(p_axis(np_, cfg["pmin"], cfg["pmax"]), dtype=torch.float64, device=tau.device)
+    pt2 = (vth * vth) * tau[:, None]
+    f00 = torch.exp(-(p[None, :] ** 2) / (2.0 * pt2)) / ((2.0 * np.pi) ** 1.5 * pt2 ** 1.5)
+    rest = torch.zeros(l0 * nx * np_ + 6 * nx, dtype=torch.float64, device=tau.device)
+    return torch.cat([f00.reshape(-1), rest])
+
+
 def build(name: str, precision: int = 0):
     if name not in WORKLOADS:
         raise KeyError(name)

@@ -1,0 +1,149 @@
+"""Adjoint of the small step (oshun_adjoint_*, 1D, m0 = 0, FP64) and the
+checkpointed torch.autograd.Function of oshun_b200.adjoint.
+
+* one step's VJP against central differences of the production forward:
+  <lam, (step(y + e d) - step(y - e d)) / 2e> = <vjp(y, lam), d>, with and
+  without the collision step (the five fields other than E_x carry no
+  cotangent and no perturbation: with m0 = 0 they never act on f or E_x);
+* the gradient of the time-integrated heat flux of one cell with respect to
+  every cell's initial temperature, through checkpointed segments, against
+  central differences (h = 1e-4 on T/T0) of the GPU forward and of the C
+  restatement of the reference's algorithm (the FP64 reference gradient),
+  and independent of the checkpoint spacing;
+* the sensitivity configuration at full size (nx = 512, lmax = 2, np = 128,
+  500 steps, checkpoints every 50, heat flux at cell 256) against central
+  differences on 16 seeded components.
+Gradient bar: max |g_i - fd_i| <= 1e-5 max |fd|.
+"""
+import numpy as np
+import pytest
+
+from oracle.cases import Deck, State
+
+pytestmark = pytest.mark.gpu
+H = 1e-4
+
+
+def _small_cfg(nx=32, np_=32, l0=2):
+    from oshun_b200 import workloads
+    cfg, tau, meta = workloads.sensitivity1d(nx=nx, l0=l0, nump=np_, length=100.0 * nx / 512)
+    return cfg, tau
+
+
+def _run(cfg):
+    from oshun_b200.adjoint import Run
+    return Run(**cfg)
+
+
+def _loss(run, cfg, tau_t, nsteps, every, cell, grad=False):
+    import torch
+    from oshun_b200 import workloads
+    from oshun_b200.adjoint import StepsWithCheckpoints, heat_flux_weight
+    w = heat_flux_weight(cfg, cell)
+    if grad:
+        tau_t = tau_t.clone().requires_grad_(True)
+        y0 = workloads.sensitivity_state(cfg, tau_t)
+        Q = StepsWithCheckpoints.apply(y0, run, nsteps, every, w)
+        Q.backward()
+        return float(Q), tau_t.grad.detach().cpu().numpy()
+    with torch.no_grad():
+        y0 = workloads.sensitivity_state(cfg, tau_t)
+        return float(StepsWithCheckpoints.apply(y0, run, nsteps, every, w)), None
+
+
+@pytest.mark.parametrize("collisions", [False, True])
+def test_step_vjp_directional(collisions):
+    import torch
+    from oshun_b200 import workloads
+    from oshun_b200.adjoint import state_layout
+    cfg, tau = _small_cfg(nx=16)
+    run = _run(cfg)
+    lay = state_layout(cfg)
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    y = workloads.sensitivity_state(cfg, torch.tensor(tau, device="cuda"))
+    f = y[lay["f"]].view(lay["fshape"])
+    scale = f[0].abs().max()
+    f[1:] = 0.05 * scale * torch.randn(f[1:].shape, generator=gen, device="cuda", dtype=torch.float64)
+    y[lay["fields"]][: cfg["numx"]] = 1e-3 * torch.randn(cfg["numx"], generator=gen, device="cuda", dtype=torch.float64)
+    d = torch.zeros_like(y)
+    d[lay["f"]] = 1e-2 * scale * torch.randn(lay["f"].stop, generator=gen, device="cuda", dtype=torch.float64)
+    d[lay["f"]].view(lay["fshape"])[0] *= 0.1          # f00 perturbation small against f00
+    d[lay["fields"]][: cfg["numx"]] = 1e-4 * torch.randn(cfg["numx"], generator=gen, device="cuda", dtype=torch.float64)
+    lam = torch.zeros_like(y)
+    lam[lay["f"]] = torch.randn(lay["f"].stop, generator=gen, device="cuda", dtype=torch.float64)
+    lam[lay["fields"]][: cfg["numx"]] = torch.randn(cfg["numx"], generator=gen, device="cuda", dtype=torch.float64)
+    clocks = (0.0, 0.0, 0.0)
+    eps = 1e-3
+    yp = run.forward(y + eps * d, clocks, collisions)
+    ym = run.forward(y - eps * d, clocks, collisions)
+    lhs = float(torch.dot(lam, yp - ym)) / (2 * eps)
+    rhs = float(torch.dot(run.vjp(y, lam, clocks, collisions), d))
+    assert abs(lhs - rhs) <= 1e-7 * (abs(lhs) + abs(rhs)), (lhs, rhs)
+
+
+def _oracle_loss(oracle, cfg, tau, nsteps, cell):
+    """the same functional through the C restatement (the reference's algorithm)"""
+    from oshun_b200 import workloads
+    from oshun_b200.adjoint import heat_flux_weight
+    d = Deck(l0=cfg["l0"], m0=0, nump=cfg["nump"], numx=cfg["numx"], numy=1, pmin=cfg["pmin"], pmax=cfg["pmax"],
+             xmin=cfg["xmin"], xmax=cfg["xmax"], dt=cfg["dt"], small_dt=cfg["small_dt"],
+             density_np=cfg["density_np"])
+    st = State(d)
+    p = d.pr()
+    st.f[0, 0] = workloads.maxwellian(p[None, :], 0.05 * np.sqrt(tau)[:, None])
+    w = heat_flux_weight(cfg, cell, device="cpu").numpy()
+    nx, np_ = cfg["numx"], cfg["nump"]
+    w1 = w[(1 * nx + cell) * np_:(1 * nx + cell + 1) * np_]
+    Q = 0.0
+    for _ in range(nsteps):
+        st = oracle.steps(st, 1, 15)
+        Q += cfg["dt"] * float(np.dot(w1, st.f[1, 0, cell].real))
+    return Q
+
+
+def test_checkpointed_gradient_small(oracle):
+    import torch
+    cfg, tau = _small_cfg()
+    run = _run(cfg)
+    nsteps, cell = 30, 16
+    tt = torch.tensor(tau, device="cuda")
+    Q, g = _loss(run, cfg, tt, nsteps, 7, cell, grad=True)
+    _, g1 = _loss(run, cfg, tt, nsteps, 1000, cell, grad=True)     # no intermediate checkpoint
+    assert np.max(np.abs(g - g1)) <= 1e-12 * np.max(np.abs(g))
+    comps = [0, 5, 11, 16, 17, 30]
+    fd, fd_ref = [], []
+    for i in comps:
+        e = np.zeros_like(tau)
+        e[i] = H
+        qp, _ = _loss(run, cfg, torch.tensor(tau + e, device="cuda"), nsteps, 7, cell)
+        qm, _ = _loss(run, cfg, torch.tensor(tau - e, device="cuda"), nsteps, 7, cell)
+        fd.append((qp - qm) / (2 * H))
+        fd_ref.append((_oracle_loss(oracle, cfg, tau + e, nsteps, cell) -
+                       _oracle_loss(oracle, cfg, tau - e, nsteps, cell)) / (2 * H))
+    fd, fd_ref = np.array(fd), np.array(fd_ref)
+    scale = np.max(np.abs(fd))
+    assert scale > 0
+    assert np.max(np.abs(g[comps] - fd)) <= 1e-5 * scale, (g[comps], fd)
+    assert np.max(np.abs(g[comps] - fd_ref)) <= 1e-5 * scale, (g[comps], fd_ref)
+
+
+def test_sensitivity_full_size():
+    import torch
+    from oshun_b200 import workloads
+    cfg, tau, meta = workloads.sensitivity1d()
+    run = _run(cfg)
+    nsteps, every, cell = 500, 50, 256
+    tt = torch.tensor(tau, device="cuda")
+    Q, g = _loss(run, cfg, tt, nsteps, every, cell, grad=True)
+    comps = sorted(np.random.default_rng(2024).choice(cfg["numx"], 16, replace=False).tolist())
+    fd = []
+    for i in comps:
+        e = np.zeros_like(tau)
+        e[i] = H
+        qp, _ = _loss(run, cfg, torch.tensor(tau + e, device="cuda"), nsteps, every, cell)
+        qm, _ = _loss(run, cfg, torch.tensor(tau - e, device="cuda"), nsteps, every, cell)
+        fd.append((qp - qm) / (2 * H))
+    fd = np.array(fd)
+    scale = np.max(np.abs(fd))
+    assert scale > 0 and np.isfinite(g).all()
+    assert np.max(np.abs(g[comps] - fd)) <= 1e-5 * scale, (g[comps], fd)
