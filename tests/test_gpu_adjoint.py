@@ -45,7 +45,7 @@ def _loss(run, cfg, tau_t, nsteps, every, cell, grad=False):
         y0 = workloads.sensitivity_state(cfg, tau_t)
         Q = StepsWithCheckpoints.apply(y0, run, nsteps, every, w)
         Q.backward()
-        return float(Q), tau_t.grad.detach().cpu().numpy()
+        return float(Q.detach()), tau_t.grad.detach().cpu().numpy()
     with torch.no_grad():
         y0 = workloads.sensitivity_state(cfg, tau_t)
         return float(StepsWithCheckpoints.apply(y0, run, nsteps, every, w)), None
