@@ -56,25 +56,36 @@ def parse():
 
 
 def dist_init():
+    """One process per GPU (torchrun env); NCCL with GPUs, gloo without (the
+    CPU tests of the replica logic)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         import datetime
 
-        import torch.distributed as dist
         import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
+def _dev():
+    import torch
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def reduce_max(x: float, ws: int) -> float:
+    """max over ranks (the timed region's length is the slowest rank's)"""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_dev())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -83,6 +94,12 @@ def barrier(ws: int):
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def replica_value(units_per_rank: float, ms_total_max: float, steps: int, ws: int) -> float:
+    """whole-job throughput of N independent replicas: every rank's units over
+    the slowest rank's time"""
+    return units_per_rank * steps * ws / (ms_total_max * 1e-3)
 
 
 # ----------------------------------------------------------------------------
@@ -308,7 +325,7 @@ def run_ours(args, ws, rank, local):
     clocks = sampler.stop()
     ms_total = reduce_max(e0.elapsed_time(e1), ws)
     ms_step = ms_total / args.steps
-    value = acct["coef_updates"] * args.steps * ws / (ms_total * 1e-3)
+    value = replica_value(acct["coef_updates"], ms_total, args.steps, ws)
 
     # ---- stage-kernel roofline: RK4-only steps (4 stage launches each) ------
     nrk = max(3, min(args.steps, 10))
@@ -455,7 +472,7 @@ def run_batch(args, ws, rank, local):
     clocks = sampler.stop()
     ms_total = reduce_max(e0.elapsed_time(e1), ws)
     ms_step = ms_total / args.steps
-    value = coefs * args.steps * ws / (ms_total * 1e-3)
+    value = replica_value(coefs, ms_total, args.steps, ws)
     assert b.status() == 0
     peak, peak_kind = measured_peaks()
     achieved = step_bytes / (ms_step * 1e-3) / 1e9
