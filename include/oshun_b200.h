@@ -171,11 +171,11 @@ int oshun_batch_step(oshun_batch b, int nsteps);
 /* OR of every problem's status word (oshun_status_flags) and bit 4 = a
  * pipeline wait of a batched launch ran out. */
 int oshun_batch_status(oshun_batch b, int* flags);
-/* Stage tiles: consumer threads per CTA (32..256, a multiple of 32, at least
+/* Stage tiles: consumer threads per CTA (32..320, a multiple of 32, at least
  * the widest padded nump of the batch) and cells per tile at most (1..8). */
 int oshun_batch_set_tiles(oshun_batch b, int stage_threads, int tile_cells);
 int oshun_batch_get_tiles(oshun_batch b, int* stage_threads, int* tile_cells);
-/* Autotuner: times every tile candidate (stage threads 128/192/256 x cells
+/* Autotuner: times every tile candidate (stage threads 128/192/256/320 x cells
  * per tile 1/2/4/8) on `steps` steps of the batch itself, keeps the fastest
  * and restores the state and clocks; returns the choice and its ms/step. */
 int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile_cells, double* ms_per_step);

@@ -1273,7 +1273,7 @@ int oshun_batch_download(oshun_batch b, int i, double* harmonics, double* fields
 }
 
 int oshun_batch_set_tiles(oshun_batch b, int stage_threads, int tile_cells) {
-    if (!b || stage_threads < 32 || stage_threads > 256 || stage_threads % 32 || tile_cells < 1 || tile_cells > 8)
+    if (!b || stage_threads < 32 || stage_threads > 320 || stage_threads % 32 || tile_cells < 1 || tile_cells > 8)
         return OSHUN_ERR_ARG;
     CK(cudaStreamSynchronize(b->stream));
     const int nc0 = b->nc, tx0 = b->tx_cap;
@@ -1385,7 +1385,7 @@ int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile
     };
     rc = save_restore(true);
     if (!rc) {
-        const int nc_c[] = {128, 192, 256};
+        const int nc_c[] = {128, 192, 256, 320};
         const int tx_c[] = {1, 2, 4, 8};
         int best_nc = b->nc, best_tx = b->tx_cap;
         double best = 1e300;

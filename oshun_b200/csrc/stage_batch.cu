@@ -9,10 +9,12 @@ namespace {
 template <typename TS, int MC>
 cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaStream_t s) {
     const SmemPlan P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth);
-    if (P.total > 227 * 1024) return cudaErrorNotSupported;
+    if (P.total > kSmemMax) return cudaErrorNotSupported;
     const int threads = nc + 64;
+    // 9-12 warps are granted 12 warps' registers (168 a thread), so one
+    // instantiation covers 257-384 threads
     if (threads <= 256) return launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
-    if (threads <= 320) return launch_pipe<MC, TS, 320, true>(a1, bw, threads, P.total, bw.nitems, s);
+    if (threads <= 384) return launch_pipe<MC, TS, 384, true>(a1, bw, threads, P.total, bw.nitems, s);
     return cudaErrorNotSupported;
 }
 
@@ -35,10 +37,10 @@ int stage_batch_coef_bytes(int elem_bytes) {
     return elem_bytes == 4 ? (int)sizeof(CoefT<float>) : (int)sizeof(CoefT<double>);
 }
 
-// nc consumer threads per CTA (a multiple of 32, <= 256); m0 of every problem <= mc
+// nc consumer threads per CTA (a multiple of 32, <= 320); m0 of every problem <= mc
 template <typename TS>
 cudaError_t launch_stage_batch(const StageArgs<TS>& a1, const BatchWork& bw, int mc, int nc, cudaStream_t s) {
-    if (nc < 32 || nc > 256 || nc % 32) return cudaErrorInvalidValue;
+    if (nc < 32 || nc > 320 || nc % 32) return cudaErrorInvalidValue;
     switch (mc) {
         case 0: return batch_mc<TS, 0>(a1, bw, nc, s);
         case 1: return batch_mc<TS, 1>(a1, bw, nc, s);

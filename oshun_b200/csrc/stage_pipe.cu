@@ -9,7 +9,7 @@ namespace oshun {
 namespace {
 
 template <int MC, typename TS, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<TS> a) {
+__global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<TS> a, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int np = a.np, nx = a.nx, ny = a.ny;
     const int np_pad = (np + 31) & ~31;
@@ -19,10 +19,10 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     const int ncw = nct >> 5;                          // consumer warps
     const int mstride = a.m0 + 1;
     const int ncoef = (a.l0 + 1) * mstride;
-    const PipeLayout L = pipe_layout(ncoef, tx, np, has_y, (int)sizeof(TS), a.m0);
+    const PipeLayout L = pipe_layout(ncoef, tx, np, has_y, (int)sizeof(TS), a.m0, D);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-    uint64_t* empty = full + kDepth;
-    uint64_t* rowfull = empty + kDepth;
+    uint64_t* empty = full + kMaxDepth;
+    uint64_t* rowfull = empty + kMaxDepth;
     uint64_t* rowempty = rowfull + 2;
     CoefT<TS>* scoef = reinterpret_cast<CoefT<TS>*>(smem + L.off_coef);
     int* splane = reinterpret_cast<int*>(smem + L.off_plane);
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         for (int i = tid; i < nd; i += blockDim.x) dst[i] = (TS)src[i];
         for (int i = tid; i < ncoef; i += blockDim.x) splane[i] = a.plane_of[i];
         if (tid == 0) {
-            for (int k = 0; k < kDepth; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
+            for (int k = 0; k < D; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
             for (int k = 0; k < 2; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 const bool x_contig = x0 > 0 && x0 + txv < nx;
                 for (int s = 0; s <= a.l0 && ok; ++s) {
                     for (int m = 0; m <= min(s, a.m0); ++m) {
-                        const int slot = issued % kDepth, j = issued / kDepth;
+                        const int slot = issued % D, j = issued / D;
                         if (j >= 1 && !mbar_wait(empty + slot, (uint32_t)((j - 1) & 1))) { ok = false; break; }
                         unsigned char* dst = slots + (size_t)slot * L.slot_bytes;
                         const unsigned char* src;
@@ -112,8 +112,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             if (!ok) {
                 atomicOr(a.err, 16);
                 // bounded drain of every copy that may still be in flight
-                for (int idx = max(0, issued - kDepth); idx < issued; ++idx)
-                    mbar_wait(full + (idx % kDepth), (uint32_t)((idx / kDepth) & 1));
+                for (int idx = max(0, issued - D); idx < issued; ++idx)
+                    mbar_wait(full + (idx % D), (uint32_t)((idx / D) & 1));
             }
         } else if (tid == nct + 32 && need_B) {
             // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     auto release = [&]() {
         __syncwarp();
         if (lane == 0) mbar_arrive(empty + slot);
-        if (++slot == kDepth) { slot = 0; phase ^= 1u; }
+        if (++slot == D) { slot = 0; phase ^= 1u; }
     };
 
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tile_iter) {
@@ -352,7 +352,7 @@ cudaError_t launch_tile(const StageArgs<TS>& a, int tx, const PipeLayout& L, cud
     const long long tiles = (long long)a.ny * ((a.nx + tx - 1) / tx);
     // one resident CTA per SM, each walking tiles blockIdx.x + k gridDim.x
     const long long blocks = tiles < sm_count() ? tiles : sm_count();
-    rk_stage_tile_kernel<MC, TS, MAXT><<<dim3((unsigned)blocks), dim3(np_pad * tx + 64), L.total, s>>>(a);
+    rk_stage_tile_kernel<MC, TS, MAXT><<<dim3((unsigned)blocks), dim3(np_pad * tx + 64), L.total, s>>>(a, L.depth);
     return cudaGetLastError();
 }
 
@@ -361,15 +361,38 @@ cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
     const int np_pad = ((a.np + 31) / 32) * 32;
     // bulk copies move whole momentum rows: 16-byte multiples for every plane type
     if ((a.np * (int)sizeof(TS)) % 16 != 0 || np_pad > 256) return cudaErrorNotSupported;
-    // consumer threads <= 192: 8 warps with the producers, 255 registers per thread
-    int tx = np_pad <= 192 ? 192 / np_pad : 1;
+    // The kernel is latency-bound: more consumer warps per SM pay even when
+    // the register cap makes the FP64 accumulators spill a little.  Registers
+    // are granted per SM sub-partition, so a CTA of 9-12 warps costs 12 warps'
+    // worth: 168 registers a thread; 13-16 warps: 128.  Consumer threads:
+    //   m0 <= 1 (<= 120 registers)              up to 448 (16 warps)
+    //   m0 <= 6, or FP32 arithmetic             up to 320 (12 warps)
+    //   FP64 with m0 >= 7 (spills at 168)       up to 192 (8 warps, 255)
+    const int budget = MC <= 1 ? 448 : (sizeof(TS) == 4 || MC <= 6) ? 320 : 192;
+    int tx = budget >= np_pad ? budget / np_pad : 1;
     if (tx > kMaxTx) tx = kMaxTx;
     if (tx > a.nx) tx = a.nx;
+    // at least one tile per SM where the grid has the cells for it
+    const long long cells = (long long)a.nx * a.ny;
+    const long long per_sm = cells / sm_count();
+    if (tx > per_sm) tx = per_sm > 1 ? (int)per_sm : 1;
     const int ncoef = (a.l0 + 1) * (a.m0 + 1);
-    const PipeLayout L = pipe_layout(ncoef, tx, a.np, a.ny > 1, (int)sizeof(TS), a.m0);
-    if (L.total > 227 * 1024) return cudaErrorNotSupported;
-    if (np_pad * tx <= 192) return launch_tile<MC, TS, 256>(a, tx, L, s);
-    return launch_tile<MC, TS, 320>(a, tx, L, s);
+    // the deepest source ring that fits (4 slots at least), else fewer cells a tile
+    PipeLayout L;
+    for (;;) {
+        int depth = kDepth;
+        L = pipe_layout(ncoef, tx, a.np, a.ny > 1, (int)sizeof(TS), a.m0, depth);
+        while (L.total > kSmemMax && depth > 4)
+            L = pipe_layout(ncoef, tx, a.np, a.ny > 1, (int)sizeof(TS), a.m0, --depth);
+        if (L.total <= kSmemMax || tx == 1) break;
+        --tx;
+    }
+    if (L.total > kSmemMax) return cudaErrorNotSupported;
+    const int threads = np_pad * tx + 64;
+    if (threads <= 256) return launch_tile<MC, TS, 256>(a, tx, L, s);
+    if (threads <= 384) return launch_tile<MC, TS, 384>(a, tx, L, s);
+    if constexpr (MC <= 1) return launch_tile<MC, TS, 512>(a, tx, L, s);
+    return cudaErrorNotSupported;
 }
 
 }  // namespace

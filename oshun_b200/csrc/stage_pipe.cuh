@@ -51,10 +51,12 @@ namespace oshun {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kDepth = 10;                    // source slots in the ring
+constexpr int kDepth = 10;                    // source slots in the ring (batched kernel; default)
+constexpr int kMaxDepth = 12;                 // ring slots the barrier area holds
 constexpr uint32_t kSuspendNs = 20000;         // sleep hint of one mbarrier try_wait
 constexpr unsigned long long kWaitNs = 1000000000ull;   // a pipeline wait gives up after 1 s
 constexpr int kMaxTx = 8;
+constexpr size_t kSmemMax = 227 * 1024;          // dynamic shared memory of one CTA
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
@@ -138,9 +140,11 @@ struct alignas(16) CoefT {
 struct PipeLayout {
     size_t off_coef, off_plane, off_sj, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
     int seg_cells;
+    int depth;   // slots in the source ring (<= kMaxDepth)
 };
-// barriers at offset 0: full[kDepth], empty[kDepth], rowfull[2], rowempty[2]
-__host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, bool has_y, int elem_bytes, int m0) {
+// barriers at offset 0: full[kMaxDepth], empty[kMaxDepth], rowfull[2], rowempty[2]
+__host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, bool has_y, int elem_bytes, int m0,
+                                                 int depth = kDepth) {
     PipeLayout L;
     L.seg_cells = tx + 2 + (has_y ? 2 * tx : 0);
     L.off_coef = 256;
@@ -151,7 +155,8 @@ __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, boo
     const size_t plane_part = (size_t)2 * L.seg_cells * np * elem_bytes;
     const size_t f00_part = (size_t)L.seg_cells * np * 8;
     L.slot_bytes = align_up(plane_part > f00_part ? plane_part : f00_part, 128);
-    L.off_rows = L.off_slots + kDepth * L.slot_bytes;
+    L.depth = depth;
+    L.off_rows = L.off_slots + (size_t)depth * L.slot_bytes;
     const size_t row0 = (size_t)tx * np * 8;
     const size_t rowl = (size_t)(1 + 2 * m0) * tx * np * elem_bytes;
     L.row_arr_bytes = align_up(row0 > rowl ? row0 : rowl, 128);
@@ -379,13 +384,14 @@ __host__ __device__ inline SmemPlan smem_plan(bool batch, int hdr_bytes, int nco
 }
 
 // resident CTAs per SM the batched kernel is compiled for: two when the
-// accumulators are few (m0 <= 1, the 1D batches), so that one CTA's tile
-// start and end latencies overlap the other's work
-template <int MC, bool BATCH>
-constexpr int batch_min_blocks() { return (BATCH && MC <= 1) ? 2 : 1; }
+// accumulators are few (m0 <= 1, the 1D batches) and the CTA has at most
+// 10 warps, so that one CTA's tile start and end latencies overlap the
+// other's work (two 12-warp CTAs would leave 80 registers a thread)
+template <int MC, int MAXT, bool BATCH>
+constexpr int batch_min_blocks() { return (BATCH && MC <= 1 && MAXT <= 320) ? 2 : 1; }
 
 template <int MC, typename TS, int MAXT, bool BATCH>
-__global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, BATCH>())
+__global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
     rk_stage_pipe_kernel(const StageArgs<TS> a1, const BatchWork bw) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;

@@ -61,7 +61,7 @@ def _batch(problems, nsteps, collide, tiles=None, autotune=False, stream=None):
         if autotune:
             before = [b.download(i) for i in range(b.n)]
             nc, tx, ms = b.autotune(steps=1)
-            assert nc in (128, 192, 256) and tx in (1, 2, 4, 8) and ms > 0
+            assert nc in (128, 192, 256, 320) and tx in (1, 2, 4, 8) and ms > 0
             after = [b.download(i) for i in range(b.n)]
             for (f0, l0), (f1, l1) in zip(before, after):
                 assert np.array_equal(f0, f1) and np.array_equal(l0, l1)
