@@ -340,7 +340,7 @@ def run_ours(args, ws, rank, local):
     achieved = acct["stage_bytes"] / (launch_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": ncu_traffic(args.workload, args.precision),
-                "peak_source": peak_kind, "kernel": "rk_stage_kernel",
+                "peak_source": peak_kind, "kernel": "rk_stage_tile_kernel (+ stage_fields_kernel)",
                 "algorithmic_bytes_per_launch": acct["stage_bytes"], "avg_launch_ms": round(launch_ms, 4)}
     step_gbs = acct["step_bytes"] / (ms_step * 1e-3) / 1e9
 
@@ -390,8 +390,9 @@ def run_ours(args, ws, rank, local):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms},
             "roofline": roofline,
-            # per step: 4 RK4 stage kernels, the clock advance, the collision kernel, the clock commit
-            "gpu_launches": 7 * args.steps,
+            # per step: 4 RK4 stages (the stage kernel and its field kernel each),
+            # the clock advance, the collision kernel, the clock commit
+            "gpu_launches": 11 * args.steps,
             "clocks": clocks,
         }
         if cpu is not None:

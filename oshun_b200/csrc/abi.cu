@@ -160,6 +160,7 @@ struct oshun_ctx {
     double* d_dense_ws = nullptr;
     int dense_blocks = 0;
     int* d_status = nullptr;
+    double* d_jw = nullptr;      // [cells][3][8] current partial sums of the pipelined stage
     Clock* d_clock = nullptr;
     double2* d_stage = nullptr;  // host-layout staging for transfers and slopes
 
@@ -279,6 +280,7 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     a.g00_s = g00_s; a.g00_inv = g00_inv; a.g00_gr = g00_gr;
     a.idx = idx; a.idy = idy;
     a.seq = d_seq; a.nh = nh; a.err = d_status;
+    a.jw = d_jw;
     (void)out_set;
     return a;
 }
@@ -565,7 +567,7 @@ void free_ctx(oshun_ctx* h) {
     for (int i = 0; i < 4; ++i) { cudaFree(h->f00[i]); cudaFree(h->pl[i]); cudaFree(h->fld[i]); }
     cudaFree(h->d_coef); cudaFree(h->d_plane_of); cudaFree(h->d_plane_l); cudaFree(h->d_plane_m);
     cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
-    cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage);
+    cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage); cudaFree(h->d_jw);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -620,6 +622,8 @@ int oshun_create(const oshun_cfg* cfg, oshun_handle* out) {
     }
     CKF(cudaMalloc(&h->d_status, sizeof(int) * 4));
     CKF(cudaMemset(h->d_status, 0, sizeof(int) * 4));
+    CKF(cudaMalloc(&h->d_jw, sizeof(double) * 24 * h->cells));
+    CKF(cudaMemset(h->d_jw, 0, sizeof(double) * 24 * h->cells));
     CKF(cudaMalloc(&h->d_clock, sizeof(Clock)));
     Clock ck{h->t, h->t_ee, h->t_eb};
     CKF(cudaMemcpy(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice));

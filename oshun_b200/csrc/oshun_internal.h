@@ -62,6 +62,7 @@ struct StageArgs {
     int nh;
     int* err;             // error word (bit 4: a pipeline wait timed out)
     const void* coef_ts;  // coupling table in the arithmetic type (batched launches)
+    double* jw;           // [cells][3][8]: per-warp partial sums of Jx, Re Jy, Im Jy (single-problem pipeline)
 };
 
 struct CollideArgs {

@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     uint64_t* rowempty = rowfull + 2;
     CoefT<TS>* scoef = reinterpret_cast<CoefT<TS>*>(smem + L.off_coef);
     int* splane = reinterpret_cast<int*>(smem + L.off_plane);
-    double* sj = reinterpret_cast<double*>(smem + L.off_sj);   // [2 tiles][3][tx][8 warps]
+    TS* sfld = reinterpret_cast<TS*>(smem + L.off_fld);      // [2 tiles][6][tx]: the tile's E and B
     unsigned char* slots = smem + L.off_slots;
     unsigned char* rows = smem + L.off_rows;
     const bool need_B = a.mode != 1;
@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
             int issued = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            int ti = 0;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++ti) {
                 const int y = tile / tiles_x;
                 const int x0 = (tile - y * tiles_x) * tx;
                 const int txv = min(tx, nx - x0);
@@ -130,6 +131,12 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                     unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
                     const uint32_t nb = need_A ? 2 : 1;
                     if (t == 0) {
+                        // the tile's fields travel with row 0: stored before the
+                        // arrive below, whose release orders them for the consumers;
+                        // the buffer of tile ti - 2 was read at that tile's start
+                        TS* fd = sfld + (size_t)(ti & 1) * 6 * tx;
+                        for (int f = 0; f < 6; ++f)
+                            for (int cc = 0; cc < txv; ++cc) fd[f * tx + cc] = ldg(a.fld_in + f * a.cells + base_cell + cc);
                         const uint32_t b = (uint32_t)txv * np * 8;
                         mbar_expect_tx(rowfull + rb, nb * b);
                         bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
@@ -195,11 +202,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         const bool cv = c < txv;
         const bool pv = cv && pin;
         const int cc = cv ? c : 0;
-        const long long row = (long long)y * nx;
-        const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
-        const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
         const int xc = x0 + cc;
-        const long long cell = row + xc;
+        const long long cell = (long long)y * nx + xc;
 
         Nb nb;
         nb.ctr = (1 + cc) * np + pc;
@@ -212,12 +216,24 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         const int roff = cc * np + pc;          // this point inside a staged row
 
         Th<TS> th;
-        th.ex = ldg(a.fld_in + cell);
-        th.ey = ldg(a.fld_in + a.cells + cell);
-        th.ez = ldg(a.fld_in + 2 * a.cells + cell);
-        th.bx = ldg(a.fld_in + 3 * a.cells + cell);
-        th.by = ldg(a.fld_in + 4 * a.cells + cell);
-        th.bz = ldg(a.fld_in + 5 * a.cells + cell);
+        if (need_B) {
+            // the row warp staged this tile's fields with its row 0
+            const int rb = rows_used & 1;
+            if (!dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
+                atomicOr(a.err, 16);
+                dead = true;
+            }
+            const TS* fd = sfld + (size_t)(tile_iter & 1) * 6 * tx + cc;
+            th.ex = fd[0]; th.ey = fd[tx]; th.ez = fd[2 * tx];
+            th.bx = fd[3 * tx]; th.by = fd[4 * tx]; th.bz = fd[5 * tx];
+        } else {
+            th.ex = ldg(a.fld_in + cell);
+            th.ey = ldg(a.fld_in + a.cells + cell);
+            th.ez = ldg(a.fld_in + 2 * a.cells + cell);
+            th.bx = ldg(a.fld_in + 3 * a.cells + cell);
+            th.by = ldg(a.fld_in + 4 * a.cells + cell);
+            th.bz = ldg(a.fld_in + 5 * a.cells + cell);
+        }
         th.is0 = pc == 0;
         th.exg = th.is0 ? TS(0) : th.ex;
         th.eyg = th.is0 ? TS(0) : th.ey;
@@ -306,9 +322,10 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         }
         epilogue(a.l0);
 
-        // per-cell current: warp sums, then warps in order (deterministic);
-        // the partial sums of consecutive tiles alternate between two buffers
-        double* sjt = sj + (size_t)(tile_iter & 1) * 3 * tx * 8;
+        // per-cell current: warp sums to global; stage_fields_kernel adds the
+        // warps of a cell in order (deterministic) and updates E and B.  No
+        // barrier joins the consumer warps: a warp whose wait ran out stops on
+        // its own and the others' waits end by their own limits.
         const int warp_in_cell = p >> 5;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
@@ -316,27 +333,37 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             jyr += __shfl_xor_sync(kFull, jyr, off);
             jyi += __shfl_xor_sync(kFull, jyi, off);
         }
-        if (lane == 0) {
-            sjt[(0 * tx + c) * 8 + warp_in_cell] = jx;
-            sjt[(1 * tx + c) * 8 + warp_in_cell] = jyr;
-            sjt[(2 * tx + c) * 8 + warp_in_cell] = jyi;
-        }
-        // every consumer leaves the tile loop together once any wait ran out
-        dead = consumer_sync_or(nct, dead);
-        if (p == 0 && cv && !dead) {
-            double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
-            const int nw = np_pad >> 5;
-            for (int w = 0; w < nw; ++w) {
-                Jx += sjt[(0 * tx + c) * 8 + w];
-                Jyr += sjt[(1 * tx + c) * 8 + w];
-                Jyi += sjt[(2 * tx + c) * 8 + w];
-            }
-            const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
-            const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
-            field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+        if (lane == 0 && cv && !dead) {
+            double* jc = a.jw + cell * 24 + warp_in_cell;
+            jc[0] = jx;
+            jc[8] = jyr;
+            jc[16] = jyi;
         }
         if (dead) break;
     }
+}
+
+// E and B of every cell from the current partial sums of the stage kernel
+// (Ampere and Faraday on the staggered-free centred grid, then the RK update)
+template <typename TS>
+__global__ void __launch_bounds__(256) stage_fields_kernel(const StageArgs<TS> a, const int nw) {
+    const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (cell >= a.cells) return;
+    const int nx = a.nx, ny = a.ny;
+    const int y = (int)(cell / nx), xc = (int)(cell - (long long)y * nx);
+    const long long row = (long long)y * nx;
+    const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
+    const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
+    const double* jc = a.jw + cell * 24;
+    double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
+    for (int w = 0; w < nw; ++w) {
+        Jx += jc[w];
+        Jyr += jc[8 + w];
+        Jyi += jc[16 + w];
+    }
+    const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
+    const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
+    field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
 }
 
 template <int MC, typename TS, int MAXT>
@@ -353,6 +380,9 @@ cudaError_t launch_tile(const StageArgs<TS>& a, int tx, const PipeLayout& L, cud
     // one resident CTA per SM, each walking tiles blockIdx.x + k gridDim.x
     const long long blocks = tiles < sm_count() ? tiles : sm_count();
     rk_stage_tile_kernel<MC, TS, MAXT><<<dim3((unsigned)blocks), dim3(np_pad * tx + 64), L.total, s>>>(a, L.depth);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    stage_fields_kernel<TS><<<dim3((unsigned)((a.cells + 255) / 256)), dim3(256), 0, s>>>(a, np_pad >> 5);
     return cudaGetLastError();
 }
 
@@ -362,13 +392,14 @@ cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
     // bulk copies move whole momentum rows: 16-byte multiples for every plane type
     if ((a.np * (int)sizeof(TS)) % 16 != 0 || np_pad > 256) return cudaErrorNotSupported;
     // The kernel is latency-bound: more consumer warps per SM pay even when
-    // the register cap makes the FP64 accumulators spill a little.  Registers
-    // are granted per SM sub-partition, so a CTA of 9-12 warps costs 12 warps'
+    // the register cap makes the accumulators spill a little.  Registers are
+    // granted per SM sub-partition, so a CTA of 9-12 warps costs 12 warps'
     // worth: 168 registers a thread; 13-16 warps: 128.  Consumer threads:
-    //   m0 <= 1 (<= 120 registers)              up to 448 (16 warps)
-    //   m0 <= 6, or FP32 arithmetic             up to 320 (12 warps)
+    //   m0 <= 1, or FP32 with m0 <= 6           up to 448 (16 warps)
+    //   FP64 with m0 <= 6, FP32 with m0 >= 7    up to 320 (12 warps)
     //   FP64 with m0 >= 7 (spills at 168)       up to 192 (8 warps, 255)
-    const int budget = MC <= 1 ? 448 : (sizeof(TS) == 4 || MC <= 6) ? 320 : 192;
+    constexpr bool f32 = sizeof(TS) == 4;
+    constexpr int budget = (MC <= 1 || (f32 && MC <= 6)) ? 448 : (f32 || MC <= 6) ? 320 : 192;
     int tx = budget >= np_pad ? budget / np_pad : 1;
     if (tx > kMaxTx) tx = kMaxTx;
     if (tx > a.nx) tx = a.nx;
@@ -391,7 +422,7 @@ cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
     const int threads = np_pad * tx + 64;
     if (threads <= 256) return launch_tile<MC, TS, 256>(a, tx, L, s);
     if (threads <= 384) return launch_tile<MC, TS, 384>(a, tx, L, s);
-    if constexpr (MC <= 1) return launch_tile<MC, TS, 512>(a, tx, L, s);
+    if constexpr (budget == 448) return launch_tile<MC, TS, 512>(a, tx, L, s);
     return cudaErrorNotSupported;
 }
 

@@ -138,7 +138,7 @@ struct alignas(16) CoefT {
 
 // shared-memory layout (host and device agree)
 struct PipeLayout {
-    size_t off_coef, off_plane, off_sj, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
+    size_t off_coef, off_plane, off_sj, off_fld, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
     int seg_cells;
     int depth;   // slots in the source ring (<= kMaxDepth)
 };
@@ -150,7 +150,9 @@ __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, boo
     L.off_coef = 256;
     L.off_plane = align_up(L.off_coef + (size_t)16 * elem_bytes * ncoef, 16);
     L.off_sj = align_up(L.off_plane + sizeof(int) * (size_t)ncoef, 16);
-    L.off_slots = align_up(L.off_sj + sizeof(double) * 2 * 3 * (size_t)tx * 8, 128);
+    // fields of the tile's cells, [2 tiles][6][tx] (single-problem kernel)
+    L.off_fld = align_up(L.off_sj + sizeof(double) * 2 * 3 * (size_t)tx * 8, 16);
+    L.off_slots = align_up(L.off_fld + sizeof(double) * 2 * 6 * (size_t)tx, 128);
     // a slot holds one harmonic: Re and Im planes of the TS type, or the FP64 f00 plane
     const size_t plane_part = (size_t)2 * L.seg_cells * np * elem_bytes;
     const size_t f00_part = (size_t)L.seg_cells * np * 8;
