@@ -252,8 +252,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             for (int m = 0; m <= MC; ++m) { R[r][m] = 0; I[r][m] = 0; }
         double jx = 0.0, jyr = 0.0, jyi = 0.0;
 
-        // RK epilogue of target row t from the staged Y0/Y rows
-        auto epilogue = [&](const int t) {
+        // RK epilogue of target row t (slopes Rt, It) from the staged Y0/Y rows
+        auto epilogue = [&](const int t, const TS (&Rt)[MC + 1], const TS (&It)[MC + 1]) {
             const int rb = rows_used & 1;
             if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
                 atomicOr(a.err, 16);
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             if (!dead && pv) {
                 const unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
                 if (t == 0) {
-                    const double k = (double)R[0][0];
+                    const double k = (double)Rt[0];
                     if (a.mode == 1) {
                         a.f00_out[o] = k;
                     } else {
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 } else {
                     const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
                     const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
-                    store_row<MC, TS>(a, min(t, a.m0), zero, R[0], I[0], a.pl_out ? a.pl_out + g0 : nullptr,
+                    store_row<MC, TS>(a, min(t, a.m0), zero, Rt, It, a.pl_out ? a.pl_out + g0 : nullptr,
                                       a.pl_A + g0, reinterpret_cast<const TS*>(base) + roff,
                                       reinterpret_cast<const TS*>(base + L.row_arr_bytes) + roff, rstride);
                 }
@@ -285,16 +285,21 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             ++rows_used;
         };
 
-        // source row 0: f00
+        // target row t lives in R[t % 3], I[t % 3]: source row s adds into
+        // rows s-1, s, s+1, then row s-1 is finished, stored and cleared for
+        // row s+2, with no register moves between rows
+        // source row 0: f00 into row 1
         acquire();
         if (!dead) {
             const double* sb = reinterpret_cast<const double*>(slots + (size_t)slot * L.slot_bytes);
-            couple_f00<MC, TS>(R, I, scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
+            couple_f00_row<MC, TS>(R[1], I[1], scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
         }
         release();
-        rotate<MC, TS>(R, I);
 
-        for (int s = 1; s <= a.l0; ++s) {
+        // source row s, K = s % 3
+        auto source_row = [&](auto kcst, const int s) {
+            constexpr int K = decltype(kcst)::value;
+            constexpr int KM = (K + 2) % 3, KP = (K + 1) % 3;
             const CoefT<TS>* crow = scoef + s * mstride;
             const int mtop = min(s, a.m0);
             static_for<MC + 1>([&](auto mcst) {
@@ -303,7 +308,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * L.slot_bytes);
-                    couple_src<MC, m, TS>(R, I, crow[m], sb, seg, nb, th);
+                    couple_src3<MC, m, TS>(R[KM], R[K], R[KP], I[KM], I[K], I[KP], crow[m], sb, seg, nb, th);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             if constexpr (m == 0) {
@@ -317,10 +322,20 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 }
                 release();
             });
-            epilogue(s - 1);
-            rotate<MC, TS>(R, I);
+            epilogue(s - 1, R[KM], I[KM]);
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) { R[KM][m] = 0; I[KM][m] = 0; }
+        };
+        for (int s0 = 1; s0 <= a.l0; s0 += 3) {
+            source_row(std::integral_constant<int, 1>{}, s0);
+            if (s0 + 1 <= a.l0) source_row(std::integral_constant<int, 2>{}, s0 + 1);
+            if (s0 + 2 <= a.l0) source_row(std::integral_constant<int, 0>{}, s0 + 2);
         }
-        epilogue(a.l0);
+        switch (a.l0 % 3) {
+            case 0: epilogue(a.l0, R[0], I[0]); break;
+            case 1: epilogue(a.l0, R[1], I[1]); break;
+            default: epilogue(a.l0, R[2], I[2]); break;
+        }
 
         // per-cell current: warp sums to global; stage_fields_kernel adds the
         // warps of a cell in order (deterministic) and updates E and B.  No

@@ -191,11 +191,12 @@ __device__ __forceinline__ void static_for(F&& f) {
     static_for_impl<N>(f, std::make_integer_sequence<int, N>{});
 }
 
-// couplings of source (s, M), s >= 1, into target rows s-1 (R[0]), s (R[1]), s+1 (R[2])
+// couplings of source (s, M), s >= 1, into target rows s-1 (R0, I0), s (R1, I1), s+1 (R2, I2)
 template <int MC, int M, typename TS>
-__device__ __forceinline__ void couple_src(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1], const CoefT<TS>& c,
-                                           const TS* __restrict__ sb, const int seg, const Nb& nb,
-                                           const Th<TS>& th) {
+__device__ __forceinline__ void couple_src3(TS (&R0)[MC + 1], TS (&R1)[MC + 1], TS (&R2)[MC + 1],
+                                            TS (&I0)[MC + 1], TS (&I1)[MC + 1], TS (&I2)[MC + 1],
+                                            const CoefT<TS>& c, const TS* __restrict__ sb, const int seg,
+                                            const Nb& nb, const Th<TS>& th) {
     constexpr bool UP = M + 1 <= MC;
     constexpr bool DN = M >= 1;
     const TS ipx = th.invp * c.invpax;
@@ -221,23 +222,23 @@ __device__ __forceinline__ void couple_src(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1
     // Ex and x advection: (s+1, M), (s-1, M)
     {
         const TS cg = c.ex_g * th.exg, ch = c.ex_h * th.ex;
-        R[2][M] += cg * Gr + c.ax_p * dxr;
-        R[0][M] += ch * Hr + c.ax_m * dxr;
+        R2[M] += cg * Gr + c.ax_p * dxr;
+        R0[M] += ch * Hr + c.ax_m * dxr;
         if constexpr (DN) {
-            I[2][M] += cg * Gi + c.ax_p * dxi;
-            I[0][M] += ch * Hi + c.ax_m * dxi;
+            I2[M] += cg * Gi + c.ax_p * dxi;
+            I0[M] += ch * Hi + c.ax_m * dxi;
         }
     }
     if constexpr (UP) {
         // Em G -> (s+1, M+1), Em H -> (s-1, M+1), y advection, (Bz + iBy)/2 f -> (s, M+1)
         const TS gy = c.em_g * th.eyg, gz = c.em_g * th.ezg;
         const TS hy = c.em_h * th.ey, hz = c.em_h * th.ez;
-        R[2][M + 1] += gy * Gr + gz * Gi + c.ay_pp * dyr;
-        I[2][M + 1] += gy * Gi - gz * Gr + c.ay_pp * dyi;
-        R[0][M + 1] += hy * Hr + hz * Hi + c.ay_mp * dyr;
-        I[0][M + 1] += hy * Hi - hz * Hr + c.ay_mp * dyi;
-        R[1][M + 1] += th.hbz * fr - th.hby * fi;
-        I[1][M + 1] += th.hbz * fi + th.hby * fr;
+        R2[M + 1] += gy * Gr + gz * Gi + c.ay_pp * dyr;
+        I2[M + 1] += gy * Gi - gz * Gr + c.ay_pp * dyi;
+        R0[M + 1] += hy * Hr + hz * Hi + c.ay_mp * dyr;
+        I0[M + 1] += hy * Hi - hz * Hr + c.ay_mp * dyi;
+        R1[M + 1] += th.hbz * fr - th.hby * fi;
+        I1[M + 1] += th.hbz * fi + th.hby * fr;
     }
     if constexpr (DN) {
         // Ep H -> (s-1, M-1), Ep G -> (s+1, M-1), y advection, -i M Bx f -> (s, M),
@@ -246,25 +247,32 @@ __device__ __forceinline__ void couple_src(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1
         const TS qy = c.ep_g * th.eyg, qz = c.ep_g * th.ezg;
         const TS cz = c.b_m * th.bz, cy = c.b_m * th.by;
         const TS mb = TS(M) * th.bx;
-        R[0][M - 1] += py * Hr - pz * Hi + c.ay_mm * dyr;
-        R[2][M - 1] += qy * Gr - qz * Gi + c.ay_pm * dyr;
-        R[1][M - 1] += cz * fr + cy * fi;
-        R[1][M] += mb * fi;
-        I[1][M] -= mb * fr;
+        R0[M - 1] += py * Hr - pz * Hi + c.ay_mm * dyr;
+        R2[M - 1] += qy * Gr - qz * Gi + c.ay_pm * dyr;
+        R1[M - 1] += cz * fr + cy * fi;
+        R1[M] += mb * fi;
+        I1[M] -= mb * fr;
         if constexpr (M >= 2) {
-            I[0][M - 1] += py * Hi + pz * Hr + c.ay_mm * dyi;
-            I[2][M - 1] += qy * Gi + qz * Gr + c.ay_pm * dyi;
-            I[1][M - 1] += cz * fi - cy * fr;
+            I0[M - 1] += py * Hi + pz * Hr + c.ay_mm * dyi;
+            I2[M - 1] += qy * Gi + qz * Gr + c.ay_pm * dyi;
+            I1[M - 1] += cz * fi - cy * fr;
         }
     }
+}
+
+template <int MC, int M, typename TS>
+__device__ __forceinline__ void couple_src(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1], const CoefT<TS>& c,
+                                           const TS* __restrict__ sb, const int seg, const Nb& nb,
+                                           const Th<TS>& th) {
+    couple_src3<MC, M, TS>(R[0], R[1], R[2], I[0], I[1], I[2], c, sb, seg, nb, th);
 }
 
 // couplings of the f00 source into row 1 (R[2]); G00 at p = 0 from the
 // extrapolated f00(p=0) (OSHUN-1/def-VlasovMax.cpp:520-535)
 template <int MC, typename TS>
-__device__ __forceinline__ void couple_f00(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1], const CoefT<TS>& c,
-                                           const double* __restrict__ sb, const Nb& nb, const Th<TS>& th,
-                                           const double g00_s, const double g00_inv, const double g00_gr) {
+__device__ __forceinline__ void couple_f00_row(TS (&R2)[MC + 1], TS (&I2)[MC + 1], const CoefT<TS>& c,
+                                               const double* __restrict__ sb, const Nb& nb, const Th<TS>& th,
+                                               const double g00_s, const double g00_inv, const double g00_gr) {
     const TS fr = (TS)sb[nb.ctr], frm = (TS)sb[nb.pm], frp = (TS)sb[nb.pp];
     const TS dxr = (TS)(sb[nb.xm] - sb[nb.xp]) * th.vr;
     const TS dyr = (TS)(sb[nb.ym] - sb[nb.yp]) * th.vr;
@@ -274,12 +282,19 @@ __device__ __forceinline__ void couple_f00(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1
         Gr = (frp - f00x) * (TS)g00_gr;
     }
     const TS cg = c.ex_g * th.ex;
-    R[2][0] += cg * Gr + c.ax_p * dxr;
+    R2[0] += cg * Gr + c.ax_p * dxr;
     if constexpr (MC >= 1) {
         const TS gy = c.em_g * th.ey, gz = c.em_g * th.ez;
-        R[2][1] += gy * Gr + c.ay_pp * dyr;
-        I[2][1] -= gz * Gr;
+        R2[1] += gy * Gr + c.ay_pp * dyr;
+        I2[1] -= gz * Gr;
     }
+}
+
+template <int MC, typename TS>
+__device__ __forceinline__ void couple_f00(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1], const CoefT<TS>& c,
+                                           const double* __restrict__ sb, const Nb& nb, const Th<TS>& th,
+                                           const double g00_s, const double g00_inv, const double g00_gr) {
+    couple_f00_row<MC, TS>(R[2], I[2], c, sb, nb, th, g00_s, g00_inv, g00_gr);
 }
 
 template <int MC, typename TS>
