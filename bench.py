@@ -502,7 +502,9 @@ def run_batch(args, ws, rank, local):
         if r:
             cpu = {"value": r[0], "unit": UNIT, "cores": min(8, os.cpu_count() or 1), "kind": r[1], "sample": r[2]}
     if rank == 0:
-        nsteps_groups = 4 + 2 + len({(c["nump"] + 31) // 32 for c, _, _, col in probs if col})
+        # per step: 4 batched stages (stage kernel + field kernel each), 2 clock
+        # kernels, one collision launch per group of equal ceil(nump/32)
+        nsteps_groups = 8 + 2 + len({(c["nump"] + 31) // 32 for c, _, _, col in probs if col})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",

@@ -1019,6 +1019,7 @@ BatchWork batch_work(const oshun_batch_ctx* b, int c, int k) {
     bw.slot_bytes = (int)b->slot_bytes;
     bw.row_arr_bytes = (int)b->row_arr_bytes;
     bw.row_depth = b->row_depth;
+    bw.nprobs = (int)b->P.size();
     return bw;
 }
 

@@ -120,6 +120,7 @@ struct BatchWork {
     int hdr_bytes;                // slot header: the descriptor
     int slot_bytes, row_arr_bytes;   // largest slot / staged-row array of the batch
     int row_depth;                // staged-row ring depth (2..8)
+    int nprobs;                   // problems of the batch
 };
 // batched stage kernel (stage_batch.cu); nc consumer threads per CTA
 template <typename TS>

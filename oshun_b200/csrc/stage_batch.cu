@@ -13,9 +13,13 @@ cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaS
     const int threads = nc + 64;
     // 9-12 warps are granted 12 warps' registers (168 a thread), so one
     // instantiation covers 257-384 threads
-    if (threads <= 256) return launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
-    if (threads <= 384) return launch_pipe<MC, TS, 384, true>(a1, bw, threads, P.total, bw.nitems, s);
-    return cudaErrorNotSupported;
+    cudaError_t e = cudaErrorNotSupported;
+    if (threads <= 256) e = launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
+    else if (threads <= 384) e = launch_pipe<MC, TS, 384, true>(a1, bw, threads, P.total, bw.nitems, s);
+    if (e != cudaSuccess) return e;
+    // E and B of every problem from the stage's current partial sums
+    stage_fields_batch_kernel<TS><<<dim3((unsigned)bw.nprobs), dim3(128), 0, s>>>(bw.probs, bw.desc_bytes);
+    return cudaGetLastError();
 }
 
 }  // namespace

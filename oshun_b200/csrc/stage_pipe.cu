@@ -359,26 +359,11 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
 }
 
 // E and B of every cell from the current partial sums of the stage kernel
-// (Ampere and Faraday on the staggered-free centred grid, then the RK update)
+// (Ampere and Faraday with centred differences, then the RK update)
 template <typename TS>
 __global__ void __launch_bounds__(256) stage_fields_kernel(const StageArgs<TS> a, const int nw) {
     const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (cell >= a.cells) return;
-    const int nx = a.nx, ny = a.ny;
-    const int y = (int)(cell / nx), xc = (int)(cell - (long long)y * nx);
-    const long long row = (long long)y * nx;
-    const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
-    const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
-    const double* jc = a.jw + cell * 24;
-    double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
-    for (int w = 0; w < nw; ++w) {
-        Jx += jc[w];
-        Jyr += jc[8 + w];
-        Jyi += jc[16 + w];
-    }
-    const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
-    const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
-    field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+    if (cell < a.cells) fields_cell(a, cell, nw);
 }
 
 template <int MC, typename TS, int MAXT>

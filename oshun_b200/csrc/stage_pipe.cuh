@@ -109,24 +109,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
-__device__ __forceinline__ void consumer_sync(int nthreads) {
-    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
-}
-// consumer barrier that also ORs a flag over the consumer threads: a thread
-// whose pipeline wait ran out makes every consumer leave together, so no
-// consumer is left waiting on this barrier for threads that have gone
-__device__ __forceinline__ bool consumer_sync_or(int nthreads, bool flag) {
-    uint32_t out;
-    asm volatile(
-        "{\n\t.reg .pred Pin, Pout;\n\t"
-        "setp.ne.u32 Pin, %1, 0;\n\t"
-        "bar.red.or.pred Pout, 1, %2, Pin;\n\t"
-        "selp.u32 %0, 1, 0, Pout;\n\t}"
-        : "=r"(out)
-        : "r"((uint32_t)flag), "r"(nthreads)
-        : "memory");
-    return out != 0;
-}
 
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -138,7 +120,7 @@ struct alignas(16) CoefT {
 
 // shared-memory layout (host and device agree)
 struct PipeLayout {
-    size_t off_coef, off_plane, off_sj, off_fld, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
+    size_t off_coef, off_plane, off_fld, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
     int seg_cells;
     int depth;   // slots in the source ring (<= kMaxDepth)
 };
@@ -149,9 +131,8 @@ __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, boo
     L.seg_cells = tx + 2 + (has_y ? 2 * tx : 0);
     L.off_coef = 256;
     L.off_plane = align_up(L.off_coef + (size_t)16 * elem_bytes * ncoef, 16);
-    L.off_sj = align_up(L.off_plane + sizeof(int) * (size_t)ncoef, 16);
     // fields of the tile's cells, [2 tiles][6][tx] (single-problem kernel)
-    L.off_fld = align_up(L.off_sj + sizeof(double) * 2 * 3 * (size_t)tx * 8, 16);
+    L.off_fld = align_up(L.off_plane + sizeof(int) * (size_t)ncoef, 16);
     L.off_slots = align_up(L.off_fld + sizeof(double) * 2 * 6 * (size_t)tx, 128);
     // a slot holds one harmonic: Re and Im planes of the TS type, or the FP64 f00 plane
     const size_t plane_part = (size_t)2 * L.seg_cells * np * elem_bytes;
@@ -260,14 +241,7 @@ __device__ __forceinline__ void couple_src3(TS (&R0)[MC + 1], TS (&R1)[MC + 1], 
     }
 }
 
-template <int MC, int M, typename TS>
-__device__ __forceinline__ void couple_src(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1], const CoefT<TS>& c,
-                                           const TS* __restrict__ sb, const int seg, const Nb& nb,
-                                           const Th<TS>& th) {
-    couple_src3<MC, M, TS>(R[0], R[1], R[2], I[0], I[1], I[2], c, sb, seg, nb, th);
-}
-
-// couplings of the f00 source into row 1 (R[2]); G00 at p = 0 from the
+// couplings of the f00 source into row 1 (R2, I2); G00 at p = 0 from the
 // extrapolated f00(p=0) (OSHUN-1/def-VlasovMax.cpp:520-535)
 template <int MC, typename TS>
 __device__ __forceinline__ void couple_f00_row(TS (&R2)[MC + 1], TS (&I2)[MC + 1], const CoefT<TS>& c,
@@ -287,23 +261,6 @@ __device__ __forceinline__ void couple_f00_row(TS (&R2)[MC + 1], TS (&I2)[MC + 1
         const TS gy = c.em_g * th.ey, gz = c.em_g * th.ez;
         R2[1] += gy * Gr + c.ay_pp * dyr;
         I2[1] -= gz * Gr;
-    }
-}
-
-template <int MC, typename TS>
-__device__ __forceinline__ void couple_f00(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1], const CoefT<TS>& c,
-                                           const double* __restrict__ sb, const Nb& nb, const Th<TS>& th,
-                                           const double g00_s, const double g00_inv, const double g00_gr) {
-    couple_f00_row<MC, TS>(R[2], I[2], c, sb, nb, th, g00_s, g00_inv, g00_gr);
-}
-
-template <int MC, typename TS>
-__device__ __forceinline__ void rotate(TS (&R)[3][MC + 1], TS (&I)[3][MC + 1]) {
-#pragma unroll
-    for (int m = 0; m <= MC; ++m) {
-        R[0][m] = R[1][m]; I[0][m] = I[1][m];
-        R[1][m] = R[2][m]; I[1][m] = I[2][m];
-        R[2][m] = 0;       I[2][m] = 0;
     }
 }
 
@@ -331,6 +288,36 @@ __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long c
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 3 * C + cell, dBx);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 4 * C + cell, dBy);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 5 * C + cell, dBz);
+}
+
+// E and B of one cell from the per-warp current partial sums of the stage
+// kernel: the warps of the cell in order (deterministic), then field_update
+template <typename TS>
+__device__ __forceinline__ void fields_cell(const StageArgs<TS>& a, const long long cell, const int nw) {
+    const int nx = a.nx, ny = a.ny;
+    const int y = (int)(cell / nx), xc = (int)(cell - (long long)y * nx);
+    const long long row = (long long)y * nx;
+    const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
+    const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
+    const double* jc = a.jw + cell * 24;
+    double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
+    for (int w = 0; w < nw; ++w) {
+        Jx += jc[w];
+        Jyr += jc[8 + w];
+        Jyi += jc[16 + w];
+    }
+    const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
+    const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
+    field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+}
+
+// the field step of every problem of a batch: one CTA per problem
+template <typename TS>
+__global__ void __launch_bounds__(128) stage_fields_batch_kernel(const unsigned char* __restrict__ probs,
+                                                                 const int desc_bytes) {
+    const StageArgs<TS>& a = *reinterpret_cast<const StageArgs<TS>*>(probs + (size_t)blockIdx.x * desc_bytes);
+    const int nw = (a.np + 31) >> 5;
+    for (long long cell = threadIdx.x; cell < a.cells; cell += blockDim.x) fields_cell(a, cell, nw);
 }
 
 // RK update of one target row's planes from its slopes and the staged Y0 (Bs)
@@ -379,20 +366,20 @@ __host__ __device__ inline int tile_cells(int np, int nx, int nc, int tx_cap) {
 
 // shared-memory plan of one launch (host and device agree)
 struct SmemPlan {
-    size_t off_cur, off_coef, off_plane, off_sj, off_slots, slot_stride, hdr, off_rows, row_arr_bytes, total;
+    size_t off_cur, off_coef, off_plane, off_slots, slot_stride, hdr, off_rows, row_arr_bytes, total;
 };
 // barriers at offset 0: full[kDepth], empty[kDepth], rowfull[kRowMax], rowempty[kRowMax]
 constexpr int kRowMax = 8;
+constexpr int kMaxConsumerWarps = 10;   // batched launches: at most 320 consumer threads
 template <typename TS>
 __host__ __device__ inline SmemPlan smem_plan(bool batch, int hdr_bytes, int ncoef, size_t slot_bytes,
                                               size_t row_arr_bytes, int row_depth = 2) {
     SmemPlan P;
     P.hdr = batch ? (size_t)hdr_bytes : 0;
-    P.off_cur = 512;                                   // batch: current item's header, two buffers
-    P.off_coef = P.off_cur + 2 * P.hdr;                // single problem: coupling table, plane map
+    P.off_cur = 512;                                   // batch: each consumer warp's copy of its item's header
+    P.off_coef = P.off_cur + kMaxConsumerWarps * P.hdr;   // single problem: coupling table, plane map
     P.off_plane = align_up(P.off_coef + (batch ? 0 : sizeof(CoefT<TS>) * (size_t)ncoef), 16);
-    P.off_sj = align_up(P.off_plane + (batch ? 0 : sizeof(int) * (size_t)ncoef), 16);
-    P.off_slots = align_up(P.off_sj + sizeof(double) * 2 * 3 * 8 * 8, 128);
+    P.off_slots = align_up(P.off_plane + (batch ? 0 : sizeof(int) * (size_t)ncoef), 128);
     P.slot_stride = align_up(P.hdr + slot_bytes, 128);
     P.off_rows = P.off_slots + kDepth * P.slot_stride;
     P.row_arr_bytes = row_arr_bytes;
@@ -432,7 +419,6 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
     uint64_t* rowempty = rowfull + kRowMax;
     // staged-row ring depth: a batch of few harmonics per row needs rows further ahead
     const int RD = BATCH ? bw.row_depth : 2;
-    double* sj = reinterpret_cast<double*>(smem + P.off_sj);   // [2 items][3][8 cells][8 warps]
     unsigned char* slots = smem + P.off_slots;
     unsigned char* rows = smem + P.off_rows;
 
@@ -590,7 +576,6 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
     int slot = 0;
     uint32_t phase = 0;
     int rows_used = 0;
-    int iter = 0;
     int* err = a1.err;
 
     auto acquire = [&]() {
@@ -626,11 +611,8 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
         const bool pv = cv && pin;
         // invalid threads read a valid point (finite data) and store nothing
         const int cc = cv ? c : 0, pc = pin ? p : 0;
-        const long long row = (long long)y * nx;
-        const long long rym = (long long)(y == 0 ? ny - 1 : y - 1) * nx;
-        const long long ryp = (long long)(y == ny - 1 ? 0 : y + 1) * nx;
         const int xc = x0 + cc;
-        const long long cell = row + xc;
+        const long long cell = (long long)y * nx + xc;
 
         Nb nb;
         nb.ctr = (1 + cc) * np + pc;
@@ -669,17 +651,17 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
             for (int m = 0; m <= MC; ++m) { R[r][m] = 0; I[r][m] = 0; }
         double jx = 0.0, jyr = 0.0, jyi = 0.0;
 
-        // RK epilogue of target row t from the staged Y0/Y rows
-        auto epilogue = [&](const int t) {
+        // RK epilogue of target row t (slopes Rt, It) from the staged Y0/Y rows
+        auto epilogue = [&](const int t, const TS (&Rt)[MC + 1], const TS (&It)[MC + 1]) {
             const int rb = rows_used % RD;
             if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used / RD) & 1))) {
                 atomicOr(err, 16);
                 dead = true;
-                }
+            }
             if (!dead && pv) {
                 const unsigned char* base = rows + (size_t)rb * 2 * P.row_arr_bytes;
                 if (t == 0) {
-                    const double k = (double)R[0][0];
+                    const double k = (double)Rt[0];
                     if (a.mode == 1) {
                         a.f00_out[o] = k;
                     } else {
@@ -692,7 +674,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                 } else {
                     const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
                     const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
-                    store_row<MC, TS>(a, min(t, a.m0), zero, R[0], I[0], a.pl_out ? a.pl_out + g0 : nullptr,
+                    store_row<MC, TS>(a, min(t, a.m0), zero, Rt, It, a.pl_out ? a.pl_out + g0 : nullptr,
                                       a.pl_A + g0, reinterpret_cast<const TS*>(base) + roff,
                                       reinterpret_cast<const TS*>(base + P.row_arr_bytes) + roff, rstride);
                 }
@@ -702,15 +684,18 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
             ++rows_used;
         };
 
-        // source row 0: f00 (already acquired)
+        // target row t lives in R[t % 3], I[t % 3] (no register moves between rows)
+        // source row 0: f00 (already acquired) into row 1
         if (!dead) {
             const double* sb = reinterpret_cast<const double*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-            couple_f00<MC, TS>(R, I, scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
+            couple_f00_row<MC, TS>(R[1], I[1], scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
         }
         release();
-        rotate<MC, TS>(R, I);
 
-        for (int s = 1; s <= a.l0; ++s) {
+        // source row s, K = s % 3
+        auto source_row = [&](auto kcst, const int s) {
+            constexpr int K = decltype(kcst)::value;
+            constexpr int KM = (K + 2) % 3, KP = (K + 1) % 3;
             const CoefT<TS>* crow = scoef + s * mstride;
             const int mtop = min(s, a.m0);
             static_for<MC + 1>([&](auto mcst) {
@@ -719,7 +704,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-                    couple_src<MC, m, TS>(R, I, crow[m], sb, seg, nb, th);
+                    couple_src3<MC, m, TS>(R[KM], R[K], R[KP], I[KM], I[K], I[KP], crow[m], sb, seg, nb, th);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             if constexpr (m == 0) {
@@ -733,14 +718,23 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                 }
                 release();
             });
-            epilogue(s - 1);
-            rotate<MC, TS>(R, I);
+            epilogue(s - 1, R[KM], I[KM]);
+#pragma unroll
+            for (int m = 0; m <= MC; ++m) { R[KM][m] = 0; I[KM][m] = 0; }
+        };
+        for (int s0 = 1; s0 <= a.l0; s0 += 3) {
+            source_row(std::integral_constant<int, 1>{}, s0);
+            if (s0 + 1 <= a.l0) source_row(std::integral_constant<int, 2>{}, s0 + 1);
+            if (s0 + 2 <= a.l0) source_row(std::integral_constant<int, 0>{}, s0 + 2);
         }
-        epilogue(a.l0);
+        switch (a.l0 % 3) {
+            case 0: epilogue(a.l0, R[0], I[0]); break;
+            case 1: epilogue(a.l0, R[1], I[1]); break;
+            default: epilogue(a.l0, R[2], I[2]); break;
+        }
 
-        // per-cell current: warp sums, then warps in order (deterministic);
-        // the partial sums of consecutive items alternate between two buffers
-        double* sjt = sj + (size_t)(iter & 1) * 3 * 8 * 8;
+        // per-cell current: warp sums to the problem's partial-sum array;
+        // the batched field kernel adds the warps of a cell in order
         const int warp_in_cell = p >> 5;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
@@ -748,39 +742,27 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
             jyr += __shfl_xor_sync(kFull, jyr, off);
             jyi += __shfl_xor_sync(kFull, jyi, off);
         }
-        if (lane == 0 && c < 8) {
-            sjt[(0 * 8 + c) * 8 + warp_in_cell] = jx;
-            sjt[(1 * 8 + c) * 8 + warp_in_cell] = jyr;
-            sjt[(2 * 8 + c) * 8 + warp_in_cell] = jyi;
-        }
-        // every consumer leaves the tile loop together once any wait ran out
-        dead = consumer_sync_or(nc, dead);
-        if (p == 0 && cv && !dead) {
-            double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
-            const int nw = np_pad >> 5;
-            for (int w = 0; w < nw; ++w) {
-                Jx += sjt[(0 * 8 + c) * 8 + w];
-                Jyr += sjt[(1 * 8 + c) * 8 + w];
-                Jyi += sjt[(2 * 8 + c) * 8 + w];
-            }
-            const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
-            const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
-            field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+        if (lane == 0 && cv && !dead) {
+            double* jc = a.jw + cell * 24 + warp_in_cell;
+            jc[0] = jx;
+            jc[8] = jyr;
+            jc[16] = jyi;
         }
     };
 
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++iter) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int tile = item_tile(it);
-        // the item's first slot (f00) carries the batch header
+        // the item's first slot (f00) carries the batch header; every consumer
+        // warp keeps its own copy, so no barrier joins the warps
         acquire();
         if constexpr (BATCH) {
-            unsigned char* cur = smem + P.off_cur + (size_t)(iter & 1) * P.hdr;
+            unsigned char* cur = smem + P.off_cur + (size_t)(tid >> 5) * P.hdr;
             if (!dead) {
                 const float4* s4 = reinterpret_cast<const float4*>(slots + (size_t)slot * P.slot_stride);
                 float4* d4 = reinterpret_cast<float4*>(cur);
-                for (int i = tid; i < (int)(P.hdr / 16); i += nc) d4[i] = s4[i];
+                for (int i = lane; i < (int)(P.hdr / 16); i += 32) d4[i] = s4[i];
             }
-            consumer_sync(nc);
+            __syncwarp();
             // the coupling table and the plane map stay in global memory (L1-resident)
             const StageArgs<TS>& ab = *reinterpret_cast<const StageArgs<TS>*>(cur);
             item(ab, reinterpret_cast<const CoefT<TS>*>(ab.coef_ts), ab.plane_of, tile);
