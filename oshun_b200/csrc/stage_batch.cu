@@ -12,9 +12,11 @@ cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaS
     if (P.total > kSmemMax) return cudaErrorNotSupported;
     const int threads = nc + 64;
     // 9-12 warps are granted 12 warps' registers (168 a thread), so one
-    // instantiation covers 257-384 threads
+    // instantiation covers 257-384 threads; with m0 <= 1 a 320-thread CTA is
+    // compiled for two per SM (102 registers)
     cudaError_t e = cudaErrorNotSupported;
     if (threads <= 256) e = launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
+    else if (MC <= 1 && threads <= 320) e = launch_pipe<MC, TS, 320, true>(a1, bw, threads, P.total, bw.nitems, s);
     else if (threads <= 384) e = launch_pipe<MC, TS, 384, true>(a1, bw, threads, P.total, bw.nitems, s);
     if (e != cudaSuccess) return e;
     // E and B of every problem from the stage's current partial sums
