@@ -245,15 +245,14 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         const double wj = pv ? wj_p : 0.0;
         const long long o = cell * np + pc;
 
-        TS R[3][MC + 1], I[3][MC + 1];
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int m = 0; m <= MC; ++m) { R[r][m] = 0; I[r][m] = 0; }
+        Acc<TS, MC> A[3];
+        acc_zero(A[0]);
+        acc_zero(A[1]);
+        acc_zero(A[2]);
         double jx = 0.0, jyr = 0.0, jyi = 0.0;
 
         // RK epilogue of target row t (slopes Rt, It) from the staged Y0/Y rows
-        auto epilogue = [&](const int t, const TS (&Rt)[MC + 1], const TS (&It)[MC + 1]) {
+        auto epilogue = [&](const int t, const Acc<TS, MC>& At) {
             const int rb = rows_used & 1;
             if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
                 atomicOr(a.err, 16);
@@ -262,7 +261,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             if (!dead && pv) {
                 const unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
                 if (t == 0) {
-                    const double k = (double)Rt[0];
+                    const double k = (double)acc_re(At, 0);
                     if (a.mode == 1) {
                         a.f00_out[o] = k;
                     } else {
@@ -275,7 +274,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 } else {
                     const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
                     const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
-                    store_row<MC, TS>(a, min(t, a.m0), zero, Rt, It, a.pl_out ? a.pl_out + g0 : nullptr,
+                    store_row<MC, TS>(a, min(t, a.m0), zero, At, a.pl_out ? a.pl_out + g0 : nullptr,
                                       a.pl_A + g0, reinterpret_cast<const TS*>(base) + roff,
                                       reinterpret_cast<const TS*>(base + L.row_arr_bytes) + roff, rstride);
                 }
@@ -292,7 +291,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         acquire();
         if (!dead) {
             const double* sb = reinterpret_cast<const double*>(slots + (size_t)slot * L.slot_bytes);
-            couple_f00_row<MC, TS>(R[1], I[1], scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
+            couple_f00<MC>(A[1], scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
         }
         release();
 
@@ -308,7 +307,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * L.slot_bytes);
-                    couple_src3<MC, m, TS>(R[KM], R[K], R[KP], I[KM], I[K], I[KP], crow[m], sb, seg, nb, th);
+                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             if constexpr (m == 0) {
@@ -322,9 +321,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 }
                 release();
             });
-            epilogue(s - 1, R[KM], I[KM]);
-#pragma unroll
-            for (int m = 0; m <= MC; ++m) { R[KM][m] = 0; I[KM][m] = 0; }
+            epilogue(s - 1, A[KM]);
+            acc_zero(A[KM]);
         };
         for (int s0 = 1; s0 <= a.l0; s0 += 3) {
             source_row(std::integral_constant<int, 1>{}, s0);
@@ -332,9 +330,9 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             if (s0 + 2 <= a.l0) source_row(std::integral_constant<int, 0>{}, s0 + 2);
         }
         switch (a.l0 % 3) {
-            case 0: epilogue(a.l0, R[0], I[0]); break;
-            case 1: epilogue(a.l0, R[1], I[1]); break;
-            default: epilogue(a.l0, R[2], I[2]); break;
+            case 0: epilogue(a.l0, A[0]); break;
+            case 1: epilogue(a.l0, A[1]); break;
+            default: epilogue(a.l0, A[2]); break;
         }
 
         // per-cell current: warp sums to global; stage_fields_kernel adds the

@@ -172,9 +172,50 @@ __device__ __forceinline__ void static_for(F&& f) {
     static_for_impl<N>(f, std::make_integer_sequence<int, N>{});
 }
 
+// Slope accumulators of one target row.  FP64: Re and Im arrays.  FP32:
+// (Re, Im) pairs, which the paired FP32 FMA of sm_100 (__ffma2_rn) updates
+// in one instruction; the Im half of m = 0 is carried along and never stored.
+template <int MC>
+struct AccD {
+    double R[MC + 1], I[MC + 1];
+};
+template <int MC>
+struct AccF {
+    float2 V[MC + 1];
+};
+template <typename TS, int MC>
+struct AccOf {
+    using type = AccD<MC>;
+};
+template <int MC>
+struct AccOf<float, MC> {
+    using type = AccF<MC>;
+};
+template <typename TS, int MC>
+using Acc = typename AccOf<TS, MC>::type;
+
+template <int MC>
+__device__ __forceinline__ double acc_re(const AccD<MC>& a, int m) { return a.R[m]; }
+template <int MC>
+__device__ __forceinline__ double acc_im(const AccD<MC>& a, int m) { return a.I[m]; }
+template <int MC>
+__device__ __forceinline__ float acc_re(const AccF<MC>& a, int m) { return a.V[m].x; }
+template <int MC>
+__device__ __forceinline__ float acc_im(const AccF<MC>& a, int m) { return a.V[m].y; }
+template <int MC>
+__device__ __forceinline__ void acc_zero(AccD<MC>& a) {
+#pragma unroll
+    for (int m = 0; m <= MC; ++m) { a.R[m] = 0.0; a.I[m] = 0.0; }
+}
+template <int MC>
+__device__ __forceinline__ void acc_zero(AccF<MC>& a) {
+#pragma unroll
+    for (int m = 0; m <= MC; ++m) a.V[m] = make_float2(0.f, 0.f);
+}
+
 // couplings of source (s, M), s >= 1, into target rows s-1 (R0, I0), s (R1, I1), s+1 (R2, I2)
 template <int MC, int M, typename TS>
-__device__ __forceinline__ void couple_src3(TS (&R0)[MC + 1], TS (&R1)[MC + 1], TS (&R2)[MC + 1],
+__device__ __forceinline__ void couple_src3_ri(TS (&R0)[MC + 1], TS (&R1)[MC + 1], TS (&R2)[MC + 1],
                                             TS (&I0)[MC + 1], TS (&I1)[MC + 1], TS (&I2)[MC + 1],
                                             const CoefT<TS>& c, const TS* __restrict__ sb, const int seg,
                                             const Nb& nb, const Th<TS>& th) {
@@ -264,6 +305,87 @@ __device__ __forceinline__ void couple_f00_row(TS (&R2)[MC + 1], TS (&I2)[MC + 1
     }
 }
 
+// the couplings on the accumulator types: FP64 through the Re/Im arrays
+template <int MC, int M>
+__device__ __forceinline__ void couple_src3(AccD<MC>& A0, AccD<MC>& A1, AccD<MC>& A2, const CoefT<double>& c,
+                                            const double* __restrict__ sb, const int seg, const Nb& nb,
+                                            const Th<double>& th) {
+    couple_src3_ri<MC, M, double>(A0.R, A1.R, A2.R, A0.I, A1.I, A2.I, c, sb, seg, nb, th);
+}
+template <int MC>
+__device__ __forceinline__ void couple_f00(AccD<MC>& A2, const CoefT<double>& c, const double* __restrict__ sb,
+                                           const Nb& nb, const Th<double>& th, const double g00_s,
+                                           const double g00_inv, const double g00_gr) {
+    couple_f00_row<MC, double>(A2.R, A2.I, c, sb, nb, th, g00_s, g00_inv, g00_gr);
+}
+
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// FP32: the same couplings on (Re, Im) pairs.  With F = (fr, fi) and
+// F' = (fi, -fr), a complex coupling (a + i b) F adds a F + b F'; the
+// m = 0 sources (M = 0) carry Im = 0.
+template <int MC, int M>
+__device__ __forceinline__ void couple_src3(AccF<MC>& A0, AccF<MC>& A1, AccF<MC>& A2, const CoefT<float>& c,
+                                            const float* __restrict__ sb, const int seg, const Nb& nb,
+                                            const Th<float>& th) {
+    constexpr bool UP = M + 1 <= MC;
+    constexpr bool DN = M >= 1;
+    const float2 m1 = bc2(-1.f);
+    const float2 vr = bc2(th.vr);
+    float2 f, fm, fp, xm, xp, ym, yp;
+    f.x = sb[nb.ctr]; fm.x = sb[nb.pm]; fp.x = sb[nb.pp];
+    xm.x = sb[nb.xm]; xp.x = sb[nb.xp]; ym.x = sb[nb.ym]; yp.x = sb[nb.yp];
+    if constexpr (DN) {
+        const float* __restrict__ si = sb + seg;
+        f.y = si[nb.ctr]; fm.y = si[nb.pm]; fp.y = si[nb.pp];
+        xm.y = si[nb.xm]; xp.y = si[nb.xp]; ym.y = si[nb.ym]; yp.y = si[nb.yp];
+    } else {
+        f.y = 0.f; fm.y = 0.f; fp.y = 0.f; xm.y = 0.f; xp.y = 0.f; ym.y = 0.f; yp.y = 0.f;
+    }
+    const float2 dx = __fmul2_rn(fma2(xp, m1, xm), vr);   // (f(x-1) - f(x+1)) v
+    const float2 dy = __fmul2_rn(fma2(yp, m1, ym), vr);
+    const float2 d = fma2(fp, m1, fm);                    // f(p-1) - f(p+1)
+    const float2 Hn = fma2(f, bc2(th.invp * c.invpax), d);
+    const float2 G = fma2(d, bc2(c.gfac), Hn);
+    const float2 H = th.is0 ? __fmul2_rn(fp, bc2(c.hp0)) : Hn;
+    // Ex and x advection: (s+1, M), (s-1, M)
+    A2.V[M] = fma2(bc2(c.ex_g * th.exg), G, fma2(bc2(c.ax_p), dx, A2.V[M]));
+    A0.V[M] = fma2(bc2(c.ex_h * th.ex), H, fma2(bc2(c.ax_m), dx, A0.V[M]));
+    if constexpr (UP || DN) {
+        const float2 Gs = make_float2(G.y, -G.x), Hs = make_float2(H.y, -H.x), Fs = make_float2(f.y, -f.x);
+        if constexpr (UP) {
+            // Em G -> (s+1, M+1), Em H -> (s-1, M+1), y advection, (Bz + iBy)/2 f -> (s, M+1)
+            A2.V[M + 1] = fma2(bc2(c.em_g * th.eyg), G,
+                               fma2(bc2(c.em_g * th.ezg), Gs, fma2(bc2(c.ay_pp), dy, A2.V[M + 1])));
+            A0.V[M + 1] = fma2(bc2(c.em_h * th.ey), H,
+                               fma2(bc2(c.em_h * th.ez), Hs, fma2(bc2(c.ay_mp), dy, A0.V[M + 1])));
+            A1.V[M + 1] = fma2(bc2(th.hbz), f, fma2(bc2(-th.hby), Fs, A1.V[M + 1]));
+        }
+        if constexpr (DN) {
+            // Ep H -> (s-1, M-1), Ep G -> (s+1, M-1), y advection, (Bz - iBy) f -> (s, M-1),
+            // -i M Bx f -> (s, M); the Im halves of m = 0 targets are never stored
+            A0.V[M - 1] = fma2(bc2(c.ep_h * th.ey), H,
+                               fma2(bc2(-(c.ep_h * th.ez)), Hs, fma2(bc2(c.ay_mm), dy, A0.V[M - 1])));
+            A2.V[M - 1] = fma2(bc2(c.ep_g * th.eyg), G,
+                               fma2(bc2(-(c.ep_g * th.ezg)), Gs, fma2(bc2(c.ay_pm), dy, A2.V[M - 1])));
+            A1.V[M - 1] = fma2(bc2(c.b_m * th.bz), f, fma2(bc2(c.b_m * th.by), Fs, A1.V[M - 1]));
+            A1.V[M] = fma2(bc2(float(M) * th.bx), Fs, A1.V[M]);
+        }
+    }
+}
+template <int MC>
+__device__ __forceinline__ void couple_f00(AccF<MC>& A2, const CoefT<float>& c, const double* __restrict__ sb,
+                                           const Nb& nb, const Th<float>& th, const double g00_s,
+                                           const double g00_inv, const double g00_gr) {
+    float R2[MC + 1], I2[MC + 1];
+#pragma unroll
+    for (int m = 0; m <= MC; ++m) { R2[m] = A2.V[m].x; I2[m] = A2.V[m].y; }
+    couple_f00_row<MC, float>(R2, I2, c, sb, nb, th, g00_s, g00_inv, g00_gr);
+#pragma unroll
+    for (int m = 0; m <= MC; ++m) A2.V[m] = make_float2(R2[m], I2[m]);
+}
+
 // field epilogue: J reduction result + Ampere/Faraday, RK update of 6 fields
 template <typename TS>
 __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long cell, long long cxm, long long cxp,
@@ -324,11 +446,11 @@ __global__ void __launch_bounds__(128) stage_fields_batch_kernel(const unsigned 
 // and Y (As); the stage form is decided once per row
 template <int MC, typename TS>
 __device__ __forceinline__ void store_row(const StageArgs<TS>& a, const int mtop, const bool zero,
-                                          const TS (&R)[MC + 1], const TS (&I)[MC + 1], TS* __restrict__ out,
+                                          const Acc<TS, MC>& K, TS* __restrict__ out,
                                           TS* __restrict__ A, const TS* __restrict__ Bs, const TS* __restrict__ As,
                                           const int rstride) {
     const long long ps = a.pstride;
-    auto k_of = [&](int m, int comp) -> TS { return zero ? TS(0) : (comp ? I[m] : R[m]); };
+    auto k_of = [&](int m, int comp) -> TS { return zero ? TS(0) : (comp ? acc_im(K, m) : acc_re(K, m)); };
     if (a.mode == 1) {
         static_for<MC + 1>([&](auto mcst) {
             constexpr int m = decltype(mcst)::value;
@@ -644,15 +766,14 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
         const double wj = pv ? ldg(a.wj + p) : 0.0;
         const long long o = cell * np + pc;
 
-        TS R[3][MC + 1], I[3][MC + 1];
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int m = 0; m <= MC; ++m) { R[r][m] = 0; I[r][m] = 0; }
+        Acc<TS, MC> A[3];
+        acc_zero(A[0]);
+        acc_zero(A[1]);
+        acc_zero(A[2]);
         double jx = 0.0, jyr = 0.0, jyi = 0.0;
 
         // RK epilogue of target row t (slopes Rt, It) from the staged Y0/Y rows
-        auto epilogue = [&](const int t, const TS (&Rt)[MC + 1], const TS (&It)[MC + 1]) {
+        auto epilogue = [&](const int t, const Acc<TS, MC>& At) {
             const int rb = rows_used % RD;
             if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used / RD) & 1))) {
                 atomicOr(err, 16);
@@ -661,7 +782,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
             if (!dead && pv) {
                 const unsigned char* base = rows + (size_t)rb * 2 * P.row_arr_bytes;
                 if (t == 0) {
-                    const double k = (double)Rt[0];
+                    const double k = (double)acc_re(At, 0);
                     if (a.mode == 1) {
                         a.f00_out[o] = k;
                     } else {
@@ -674,7 +795,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                 } else {
                     const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
                     const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
-                    store_row<MC, TS>(a, min(t, a.m0), zero, Rt, It, a.pl_out ? a.pl_out + g0 : nullptr,
+                    store_row<MC, TS>(a, min(t, a.m0), zero, At, a.pl_out ? a.pl_out + g0 : nullptr,
                                       a.pl_A + g0, reinterpret_cast<const TS*>(base) + roff,
                                       reinterpret_cast<const TS*>(base + P.row_arr_bytes) + roff, rstride);
                 }
@@ -688,7 +809,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
         // source row 0: f00 (already acquired) into row 1
         if (!dead) {
             const double* sb = reinterpret_cast<const double*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-            couple_f00_row<MC, TS>(R[1], I[1], scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
+            couple_f00<MC>(A[1], scoef[0], sb, nb, th, a.g00_s, a.g00_inv, a.g00_gr);
         }
         release();
 
@@ -704,7 +825,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-                    couple_src3<MC, m, TS>(R[KM], R[K], R[KP], I[KM], I[K], I[KP], crow[m], sb, seg, nb, th);
+                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             if constexpr (m == 0) {
@@ -718,9 +839,8 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                 }
                 release();
             });
-            epilogue(s - 1, R[KM], I[KM]);
-#pragma unroll
-            for (int m = 0; m <= MC; ++m) { R[KM][m] = 0; I[KM][m] = 0; }
+            epilogue(s - 1, A[KM]);
+            acc_zero(A[KM]);
         };
         for (int s0 = 1; s0 <= a.l0; s0 += 3) {
             source_row(std::integral_constant<int, 1>{}, s0);
@@ -728,9 +848,9 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
             if (s0 + 2 <= a.l0) source_row(std::integral_constant<int, 0>{}, s0 + 2);
         }
         switch (a.l0 % 3) {
-            case 0: epilogue(a.l0, R[0], I[0]); break;
-            case 1: epilogue(a.l0, R[1], I[1]); break;
-            default: epilogue(a.l0, R[2], I[2]); break;
+            case 0: epilogue(a.l0, A[0]); break;
+            case 1: epilogue(a.l0, A[1]); break;
+            default: epilogue(a.l0, A[2]); break;
         }
 
         // per-cell current: warp sums to the problem's partial-sum array;
