@@ -503,8 +503,13 @@ def run_batch(args, ws, rank, local):
             cpu = {"value": r[0], "unit": UNIT, "cores": min(8, os.cpu_count() or 1), "kind": r[1], "sample": r[2]}
     if rank == 0:
         # per step: 4 batched stages (stage kernel + field kernel each), 2 clock
-        # kernels, one collision launch per group of equal ceil(nump/32)
-        nsteps_groups = 8 + 2 + len({(c["nump"] + 31) // 32 for c, _, _, col in probs if col})
+        # kernels, one collision launch per group of equal ceil(nump/32) and
+        # the same side of 8 resident collision CTAs per SM (the library's grouping)
+        def ctas_per_sm(c):
+            np_, l0 = c["nump"], c["l0"]
+            smem = 8 * (4 + 4 * np_ + max(9 * np_, 2 * l0 * np_))
+            return min(16, max(1, (228 * 1024) // (smem + 1024)))
+        nsteps_groups = 8 + 2 + len({((c["nump"] + 31) // 32, ctas_per_sm(c) >= 8) for c, _, _, col in probs if col})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",

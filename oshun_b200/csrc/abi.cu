@@ -885,8 +885,9 @@ int oshun_plane_index(oshun_handle h, int l, int m, int* plane) {
 //   4 x batched RK4 stage launch (one persistent kernel each, over the
 //       (problem, tile) list of the whole batch),
 //   device clock advance,
-//   per group of problems with equal ceil(nump/32): one batched collision
-//       launch over their (problem, cell) list,
+//   per group of problems with equal ceil(nump/32) and on the same side of
+//       8 resident collision CTAs per SM: one batched collision launch over
+//       their (problem, cell) list,
 //   device clock commit.
 // The stage tiles (consumer threads per CTA, cells per tile) are chosen by
 // oshun_batch_autotune, which times each candidate on the batch itself.
@@ -1191,8 +1192,17 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
         CKB(cudaMemcpy(b->d_dt, dt.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
         CKB(cudaMemcpy(b->d_collide, b->collide.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     }
-    // collision groups by ceil(nump / 32): descriptors per state parity, (problem, cell) items
-    for (int E = 1; E <= 8; ++E) {
+    // collision groups by ceil(nump / 32) and, within one nump class, by
+    // whether a cell's shared memory allows at least 8 resident one-warp CTAs
+    // per SM (the pivots of every l take 2 l0 nump doubles), so that a few
+    // problems with large l0 do not set the footprint of all the others;
+    // descriptors per state parity, (problem, cell) items
+    auto ctas_per_sm = [](size_t smem) {
+        const size_t k = (size_t)228 * 1024 / (smem + 1024);   // 1 KB reserved per CTA
+        return (int)std::min<size_t>(16, std::max<size_t>(1, k));
+    };
+    for (int E = 1; E <= 8; ++E)
+    for (int wide = 1; wide >= 0; --wide) {
         oshun_batch_ctx::Group g;
         g.E = E;
         std::vector<CollideArgs> args[2];
@@ -1200,6 +1210,7 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
         for (int i = 0; i < n; ++i) {
             oshun_ctx* h = b->P[i];
             if (!b->collide[i] || (h->cfg.nump + 31) / 32 != E) continue;
+            if ((ctas_per_sm(collide_tri_smem_per_cell(h->cfg.nump, h->cfg.l0)) >= 8) != (wide == 1)) continue;
             const int local = (int)args[0].size();
             for (int c = 0; c < 2; ++c) {
                 const int cur0 = h->cur;
