@@ -34,18 +34,29 @@ constexpr int kCollideThreads = 128;
 //   I4[k] = sum_{i=1..k} U4[i] f[i] + U4m1[i] f[i-1]
 //   I2[k] = sum_{i=1..k} U2[i] f[i] + U2m1[i] f[i-1]
 //   J1[k] = sum_{i=k+1..n-1} U1[i] f[i] + U1m1[i] f[i-1]
-// Each lane sums a contiguous run of k, the lanes' run totals are combined
-// by a warp scan, and the lane then accumulates its run again from the
-// scanned start; the three chains are independent and interleaved.
+// Each lane sums a contiguous run of k, keeping each term in the output
+// arrays (the I4 and I2 terms at their k, the J1 term of i at i - 1, all
+// inside the lane's own run), the lanes' run totals are combined by a warp
+// scan, and the lane then accumulates its run again from the scanned start
+// out of the kept terms; the three chains are independent and interleaved.
 template <class T4, class T2, class T1>
 __device__ void warp_cumsum3(double* I4, double* I2, double* J1, int n, T4 t4, T2 t2, T1 t1) {
     const int lane = threadIdx.x & 31;
     const int E = (n + 31) >> 5;
     const int b = min(lane * E, n), e = min(b + E, n);
     double l4 = 0.0, l2 = 0.0, l1 = 0.0;
-    for (int k = b; k < e; ++k)
-        if (k > 0) { l4 += t4(k); l2 += t2(k); }
-    for (int i = b + 1; i <= e && i <= n - 1; ++i) l1 += t1(i);
+    for (int k = b; k < e; ++k) {
+        if (k > 0) {
+            const double v4 = t4(k), v2 = t2(k);
+            l4 += v4; l2 += v2;
+            I4[k] = v4; I2[k] = v2;
+        }
+        if (k + 1 <= n - 1) {
+            const double v1 = t1(k + 1);
+            l1 += v1;
+            J1[k] = v1;
+        }
+    }
     double s4 = l4, s2 = l2, s1 = l1;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -60,12 +71,12 @@ __device__ void warp_cumsum3(double* I4, double* I2, double* J1, int n, T4 t4, T
     if (lane == 0) { r4 = 0.0; r2 = 0.0; }
     if (lane == 31) r1 = 0.0;
     for (int k = b; k < e; ++k) {
-        if (k > 0) { r4 += t4(k); r2 += t2(k); }
+        if (k > 0) { r4 += I4[k]; r2 += I2[k]; }
         I4[k] = r4;
         I2[k] = r2;
     }
     for (int k = e - 1; k >= b; --k) {
-        if (k + 1 <= n - 1) r1 += t1(k + 1);
+        if (k + 1 <= n - 1) r1 += J1[k];
         J1[k] = r1;
     }
     __syncwarp();
