@@ -899,6 +899,12 @@ struct oshun_batch_ctx {
     int mc = 0;                     // template class of the largest m0
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // the collision groups run side by side on the batch's stream and these
+    // two, forked after the clock advance and joined before the clock commit
+    // (groups touch disjoint problems; a group held to few resident CTAs per
+    // SM by its shared memory leaves room for another group's CTAs)
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     int cur = 0;                    // parity of every problem's state sets
     int nc = 192, tx_cap = 8;       // stage tiles
     // stage launches
@@ -941,6 +947,11 @@ void free_batch(oshun_batch_ctx* b) {
     for (auto& g : b->groups) { cudaFree(g.d_args[0]); cudaFree(g.d_args[1]); cudaFree(g.d_items); }
     cudaFree(b->d_desc); cudaFree(b->d_coef_ts); cudaFree(b->d_items);
     cudaFree(b->d_clocks); cudaFree(b->d_dt); cudaFree(b->d_collide); cudaFree(b->d_status);
+    for (int i = 0; i < 2; ++i) {
+        if (b->side[i]) cudaStreamDestroy(b->side[i]);
+        if (b->ev_join[i]) cudaEventDestroy(b->ev_join[i]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -1039,11 +1050,30 @@ int batch_enqueue_step(oshun_batch_ctx* b, int c) {
         if (e != cudaSuccess) { set_error(std::string("batched stage launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
     }
     CK(launch_clock_advance(b->d_clocks, b->d_dt, n, b->stream));
-    for (const auto& g : b->groups) {
+    // fork: each group goes to the least loaded of the three streams, largest
+    // first (load = cells x ceil(nump/32)); join before the clock commit
+    CK(cudaEventRecord(b->ev_fork, b->stream));
+    for (int i = 0; i < 2; ++i) CK(cudaStreamWaitEvent(b->side[i], b->ev_fork, 0));
+    std::vector<int> order(b->groups.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    auto load_of = [&](int i) { return (double)b->groups[i].nitems * b->groups[i].E; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return load_of(x) > load_of(y); });
+    double load[3] = {0.0, 0.0, 0.0};
+    cudaStream_t lanes[3] = {b->stream, b->side[0], b->side[1]};
+    cudaError_t e = cudaSuccess;
+    for (int gi : order) {
+        const auto& g = b->groups[gi];
+        const int li = (int)(std::min_element(load, load + 3) - load);
+        load[li] += load_of(gi);
         CollideBatch cb{g.d_args[c ^ 1], g.d_items, g.nitems};   // the new state is parity c^1
-        cudaError_t e = launch_collide_batch(cb, g.E, b->fp32 ? 1 : 0, g.smem, b->stream);
-        if (e != cudaSuccess) { set_error(std::string("batched collision launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+        e = launch_collide_batch(cb, g.E, b->fp32 ? 1 : 0, g.smem, lanes[li]);
+        if (e != cudaSuccess) break;
     }
+    for (int i = 0; i < 2; ++i) {
+        CK(cudaEventRecord(b->ev_join[i], b->side[i]));
+        CK(cudaStreamWaitEvent(b->stream, b->ev_join[i], 0));
+    }
+    if (e != cudaSuccess) { set_error(std::string("batched collision launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
     CK(launch_clock_commit(b->d_clocks, b->d_collide, n, b->stream));
     return OSHUN_OK;
 }
@@ -1098,6 +1128,11 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
     b->fp32 = cfgs[0].precision == OSHUN_FP32_SPLIT;
     CKB(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     b->own_stream = true;
+    for (int i = 0; i < 2; ++i) {
+        CKB(cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking));
+        CKB(cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming));
+    }
+    CKB(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     const int esz = b->fp32 ? 4 : 8;
     int m0max = 0;
     for (int i = 0; i < n; ++i) {
