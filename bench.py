@@ -18,7 +18,7 @@ roofline   the fused RK4-stage kernel: algorithmic bytes per launch / its
 cpu_baseline  the reference's own code (oracle/_ref, compiled from the OSHUN
            sources) on a bounded sample of the same workload, all host cores
 
-N > 1 runs independent replicas, one per GPU (the north star is one GPU;
+N > 1 runs independent replicas, one per GPU (each workload fits one GPU and
 the path needs no collective), value = sum over ranks, time = max over ranks.
 """
 from __future__ import annotations
