@@ -920,6 +920,9 @@ struct oshun_batch_ctx {
     struct Group {
         int E = 0;
         size_t smem = 0;
+        int4* d_chunks = nullptr;   // chunked form (CTAs of `warps` cells of one problem), or none
+        long long nchunks = 0;
+        int warps = 0, tab_doubles = 0;
         CollideArgs* d_args[2] = {nullptr, nullptr};   // per parity
         int2* d_items = nullptr;
         long long nitems = 0;
@@ -944,7 +947,7 @@ void free_batch(oshun_batch_ctx* b) {
     batch_drop_graphs(b);
     for (oshun_ctx* h : b->P)
         if (h) free_ctx(h);
-    for (auto& g : b->groups) { cudaFree(g.d_args[0]); cudaFree(g.d_args[1]); cudaFree(g.d_items); }
+    for (auto& g : b->groups) { cudaFree(g.d_args[0]); cudaFree(g.d_args[1]); cudaFree(g.d_items); cudaFree(g.d_chunks); }
     cudaFree(b->d_desc); cudaFree(b->d_coef_ts); cudaFree(b->d_items);
     cudaFree(b->d_clocks); cudaFree(b->d_dt); cudaFree(b->d_collide); cudaFree(b->d_status);
     for (int i = 0; i < 2; ++i) {
@@ -1065,7 +1068,8 @@ int batch_enqueue_step(oshun_batch_ctx* b, int c) {
         const auto& g = b->groups[gi];
         const int li = (int)(std::min_element(load, load + 3) - load);
         load[li] += load_of(gi);
-        CollideBatch cb{g.d_args[c ^ 1], g.d_items, g.nitems};   // the new state is parity c^1
+        CollideBatch cb{g.d_args[c ^ 1], g.d_items, g.nitems, g.d_chunks, g.nchunks, g.warps, g.tab_doubles,
+                        (int)(g.smem / sizeof(double))};   // the new state is parity c^1
         e = launch_collide_batch(cb, g.E, b->fp32 ? 1 : 0, g.smem, lanes[li]);
         if (e != cudaSuccess) break;
     }
@@ -1260,6 +1264,45 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
             for (long long cell = 0; cell < h->cells; ++cell) items.push_back(make_int2(local, (int)cell));
         }
         if (items.empty()) continue;
+        // chunked form where it keeps at least as many warps resident: CTAs of
+        // W cells of one problem share the problem's velocity tables in shared
+        // memory (per SM: 228 KB of shared memory with 1 KB reserved per CTA,
+        // 64 K registers granted in 256-register units per warp, 32 CTAs)
+        {
+            int npmax = 0;
+            for (const auto& a : args[0]) npmax = std::max(npmax, a.np);
+            const size_t tab = 12 * (size_t)npmax, celld = g.smem / sizeof(double);
+            auto resident = [](size_t bytes, int W, int regs) {
+                const int by_smem = (int)((size_t)228 * 1024 / (bytes + 1024));
+                const int per_warp = (regs * 32 + 255) / 256 * 256;
+                const int by_regs = 65536 / (per_warp * W);
+                return W * std::min(std::min(by_smem, by_regs), 32);
+            };
+            const int f32 = b->fp32 ? 1 : 0;
+            const int plain = resident(g.smem, 1, collide_batch_regs(E, f32, 0));
+            const int rchunk = collide_batch_regs(E, f32, 1);
+            int bestW = 0, bestWarps = 0;
+            for (int W = 1; W <= 8; ++W) {
+                const size_t bytes = collide_chunk_smem(W, (int)tab, (int)celld);
+                if (bytes > (size_t)227 * 1024) break;
+                const int warps = resident(bytes, W, rchunk);
+                if (warps >= bestWarps) { bestWarps = warps; bestW = W; }
+            }
+            if (bestW > 0 && bestWarps >= plain) {
+                std::vector<int4> chunks;
+                for (size_t k = 0; k < items.size();) {
+                    const int p = items[k].x, c0 = items[k].y;
+                    int cnt = 0;
+                    while (k < items.size() && items[k].x == p && cnt < bestW) { ++k; ++cnt; }
+                    chunks.push_back(make_int4(p, c0, cnt, 0));
+                }
+                g.warps = bestW;
+                g.tab_doubles = (int)tab;
+                g.nchunks = (long long)chunks.size();
+                CKB(cudaMalloc(&g.d_chunks, sizeof(int4) * chunks.size()));
+                CKB(cudaMemcpy(g.d_chunks, chunks.data(), sizeof(int4) * chunks.size(), cudaMemcpyHostToDevice));
+            }
+        }
         b->groups.push_back(g);
         auto& gg = b->groups.back();
         gg.nitems = (long long)items.size();

@@ -882,6 +882,37 @@ __global__ void __launch_bounds__(32) collide_lane_batch_kernel(const CollideBat
     }
 }
 
+// chunked batched form: a CTA of W warps takes W cells of one problem (one
+// cell per warp) and first stages the problem's twelve velocity tables (vr,
+// U4, U4m1, U2, U2m1, U1, U1m1, U3, Qn, Pn, v^5, v^7: contiguous from vr) and
+// its arguments in shared memory, so the e-e slopes and the coefficient
+// build read them there instead of from L2
+constexpr int kArgsDoubles = (int)((sizeof(CollideArgs) + 15) / 16 * 2);
+template <typename TP, int E, int P>
+__global__ void __launch_bounds__(256, 1) collide_lane_chunk_kernel(const CollideBatch b) {
+    extern __shared__ __align__(16) double smem[];
+    CollideArgs* sa = reinterpret_cast<CollideArgs*>(smem);
+    double* tab = smem + kArgsDoubles;
+    double* work = tab + b.tab_doubles;
+    const int warp = threadIdx.x >> 5;
+    for (long long ch = blockIdx.x; ch < b.nchunks; ch += gridDim.x) {
+        const int4 c = b.chunks[ch];
+        const CollideArgs& ga = b.probs[c.x];
+        const int np = ga.np;
+        if (threadIdx.x == 0) *sa = ga;
+        for (int i = threadIdx.x; i < 12 * np; i += blockDim.x) tab[i] = ga.vr[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sa->vr = tab; sa->U4 = tab + np; sa->U4m1 = tab + 2 * np; sa->U2 = tab + 3 * np;
+            sa->U2m1 = tab + 4 * np; sa->U1 = tab + 5 * np; sa->U1m1 = tab + 6 * np; sa->U3 = tab + 7 * np;
+            sa->Qn = tab + 8 * np; sa->Pn = tab + 9 * np; sa->V5 = tab + 10 * np; sa->V7 = tab + 11 * np;
+        }
+        __syncthreads();
+        if (warp < c.z) collide_lane_cell<TP, E, P>(*sa, (long long)c.y + warp, work + (size_t)warp * b.cell_doubles);
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal) {
@@ -989,7 +1020,71 @@ __global__ void clock_commit_batch_kernel(double* clocks, const int* collide, in
 }
 }  // namespace
 
+size_t collide_chunk_smem(int warps, int tab_doubles, int cell_doubles) {
+    return sizeof(double) * ((size_t)kArgsDoubles + (size_t)tab_doubles + (size_t)warps * cell_doubles);
+}
+
+namespace {
+template <typename TP, int E>
+cudaError_t launch_lane_chunk(const CollideBatch& b, cudaStream_t st) {
+    constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
+    const size_t smem = collide_chunk_smem(b.warps, b.tab_doubles, b.cell_doubles);
+    static size_t attr = 0;
+    if (smem > attr) {
+        cudaError_t e = cudaFuncSetAttribute(collide_lane_chunk_kernel<TP, E, P>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = smem;
+    }
+    const long long blocks = b.nchunks < (1ll << 30) ? b.nchunks : (1ll << 30);
+    if (blocks < 1) return cudaSuccess;
+    collide_lane_chunk_kernel<TP, E, P><<<(unsigned)blocks, 32 * b.warps, smem, st>>>(b);
+    return cudaGetLastError();
+}
+template <typename TP, int E>
+int regs_of(int chunked) {
+    constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
+    cudaFuncAttributes fa{};
+    const cudaError_t e = chunked ? cudaFuncGetAttributes(&fa, collide_lane_chunk_kernel<TP, E, P>)
+                                  : cudaFuncGetAttributes(&fa, collide_lane_batch_kernel<TP, E, P>);
+    return e == cudaSuccess ? fa.numRegs : 255;
+}
+template <typename TP>
+int regs_e(int E, int chunked) {
+    switch (E) {
+        case 1: return regs_of<TP, 1>(chunked);
+        case 2: return regs_of<TP, 2>(chunked);
+        case 3: return regs_of<TP, 3>(chunked);
+        case 4: return regs_of<TP, 4>(chunked);
+        case 5: return regs_of<TP, 5>(chunked);
+        case 6: return regs_of<TP, 6>(chunked);
+        case 7: return regs_of<TP, 7>(chunked);
+        case 8: return regs_of<TP, 8>(chunked);
+        default: return 255;
+    }
+}
+template <typename TP>
+cudaError_t launch_lane_chunk_e(const CollideBatch& b, int E, cudaStream_t st) {
+    switch (E) {
+        case 1: return launch_lane_chunk<TP, 1>(b, st);
+        case 2: return launch_lane_chunk<TP, 2>(b, st);
+        case 3: return launch_lane_chunk<TP, 3>(b, st);
+        case 4: return launch_lane_chunk<TP, 4>(b, st);
+        case 5: return launch_lane_chunk<TP, 5>(b, st);
+        case 6: return launch_lane_chunk<TP, 6>(b, st);
+        case 7: return launch_lane_chunk<TP, 7>(b, st);
+        case 8: return launch_lane_chunk<TP, 8>(b, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
+
+int collide_batch_regs(int E, int planes_fp32, int chunked) {
+    return planes_fp32 ? regs_e<float>(E, chunked) : regs_e<double>(E, chunked);
+}
+
 cudaError_t launch_collide_batch(const CollideBatch& b, int E, int planes_fp32, size_t smem, cudaStream_t st) {
+    if (b.nchunks > 0) return planes_fp32 ? launch_lane_chunk_e<float>(b, E, st) : launch_lane_chunk_e<double>(b, E, st);
     if (planes_fp32) return launch_lane_batch_e<float>(b, E, st, smem);
     return launch_lane_batch_e<double>(b, E, st, smem);
 }

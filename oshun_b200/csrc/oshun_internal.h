@@ -99,6 +99,13 @@ struct CollideBatch {
     const CollideArgs* probs;
     const int2* items;
     long long nitems;
+    // chunked form: CTAs of `warps` warps, one chunk (problem, first cell,
+    // cells) per CTA, the problem's velocity tables staged in shared memory
+    const int4* chunks;
+    long long nchunks;
+    int warps;
+    int tab_doubles;    // 12 x the group's largest nump
+    int cell_doubles;   // work space of one cell
 };
 
 // launchers (return cudaError_t)
@@ -143,6 +150,10 @@ cudaError_t launch_rk_combine(double* out, const double* v0, double a0, const do
                               double a2, long long n, cudaStream_t st);
 // tridiagonal collision step of a batch whose problems share E = ceil(np/32) <= 8
 cudaError_t launch_collide_batch(const CollideBatch& b, int E, int planes_fp32, size_t smem, cudaStream_t s);
+// shared memory of one chunked batched-collision CTA
+size_t collide_chunk_smem(int warps, int tab_doubles, int cell_doubles);
+// registers per thread of the batched collision kernel for this E (chunked or one cell per CTA)
+int collide_batch_regs(int E, int planes_fp32, int chunked);
 // device clocks {t, t_ee, t_eb} of n problems: t += dt; after a collision step t_ee = t_eb = t
 cudaError_t launch_clock_advance(double* clocks, const double* dt, int n, cudaStream_t s);
 cudaError_t launch_clock_commit(double* clocks, const int* collide, int n, cudaStream_t s);
