@@ -18,16 +18,19 @@
 // boundaries:
 //   * the source warp streams each source harmonic's tile -- the cells, their
 //     x neighbours and their y-1/y+1 segments, every momentum point -- into a
-//     ring of kDepth slots, in (l, m) order;
+//     ring of source slots (up to kMaxDepth), in (l, m) order;
 //   * the row warp streams the RK epilogue operands (Y0 and Y of the target
-//     row about to complete) into a double-buffered row stage.
+//     row about to complete) into a double-buffered row stage (and, in the
+//     single-problem kernel, each tile's six field values with its row 0).
 // The consumers read every stencil operand from shared memory through
-// per-thread offsets fixed at kernel start; the momentum-edge rules are
-// folded into those offsets (the p+1 offset of the last point is the point
-// itself, the p-1 offset of the first point is the point itself) and the
-// G/H rules at p = 0 into zeroed field copies and one select, so the
-// per-source code has no data-dependent branches.  Their only global
-// accesses are the epilogue stores.
+// per-thread offsets fixed per tile; the momentum-edge rules are folded into
+// those offsets (the p+1 offset of the last point is the point itself, the
+// p-1 offset of the first point is the point itself) and the G/H rules at
+// p = 0 into zeroed field copies and one select, so the per-source code has
+// no data-dependent branches.  The consumer warps share no barrier: each
+// writes its per-warp sums of the current to a per-cell array, and a field
+// kernel (stage_fields_kernel / stage_fields_batch_kernel) adds them in warp
+// order and updates E and B after the stage.
 //
 // Couplings of source (l, m) at one momentum point, with G/H as in
 // MakeGH/G00 (OSHUN-1/def-VlasovMax.cpp:496-535) and the reference's Dp ends
