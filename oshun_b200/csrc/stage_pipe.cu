@@ -31,6 +31,9 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     unsigned char* rows = smem + L.off_rows;
     const bool need_B = a.mode != 1;
     const bool need_A = a.mode != 1 && !a.first;
+    // Y0 enters the update only through the stage output and the first
+    // stage's Y = Y0 + ...; the last stage (no output) reads none
+    const bool need_Y0 = need_B && (a.first || a.f00_out != nullptr);
 
     const int tid = threadIdx.x;
     const int tiles_x = (nx + tx - 1) / tx;
@@ -129,7 +132,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                     const int rb = issued & 1, k = issued >> 1;
                     if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1))) { ok = false; break; }
                     unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
-                    const uint32_t nb = need_A ? 2 : 1;
+                    const uint32_t nb = (need_Y0 ? 1 : 0) + (need_A ? 1 : 0);
                     if (t == 0) {
                         // the tile's fields travel with row 0: stored before the
                         // arrive below, whose release orders them for the consumers;
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                             for (int cc = 0; cc < txv; ++cc) fd[f * tx + cc] = ldg(a.fld_in + f * a.cells + base_cell + cc);
                         const uint32_t b = (uint32_t)txv * np * 8;
                         mbar_expect_tx(rowfull + rb, nb * b);
-                        bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
+                        if (need_Y0) bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
                         if (need_A) bulk_g2s(base + L.row_arr_bytes, a.f00_A + base_cell * np, b, rowfull + rb);
                     } else {
                         const int np_row = 1 + 2 * min(t, a.m0);
@@ -149,7 +152,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                         for (int kk = 0; kk < np_row; ++kk) {
                             const long long off = (q0 + kk) * a.pstride + base_cell * np;
                             const size_t d = (size_t)kk * tx * np * sizeof(TS);
-                            bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
+                            if (need_Y0) bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
                             if (need_A) bulk_g2s(base + L.row_arr_bytes + d, a.pl_A + off, b, rowfull + rb);
                         }
                     }

@@ -653,17 +653,19 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
             } else {
                 // row warp: Y0 (and Y) of each target row, up to RD rows ahead of its epilogue
                 const bool need_A = !a.first;
+                // Y0 enters only through the stage output and the first stage's Y
+                const bool need_Y0 = a.first || a.f00_out != nullptr;
                 const long long base_cell = row + x0;
                 long long q0 = 0;   // first plane of row t (planes in (l, m) order)
                 for (int t = 0; t <= a.l0; ++t) {
                     const int rb = issued % RD, k = issued / RD;
                     if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1))) { ok = false; break; }
                     unsigned char* base = rows + (size_t)rb * 2 * P.row_arr_bytes;
-                    const uint32_t nb = need_A ? 2 : 1;
+                    const uint32_t nb = (need_Y0 ? 1 : 0) + (need_A ? 1 : 0);
                     if (t == 0) {
                         const uint32_t b = (uint32_t)txv * np * 8;
                         mbar_expect_tx(rowfull + rb, nb * b);
-                        bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
+                        if (need_Y0) bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
                         if (need_A) bulk_g2s(base + P.row_arr_bytes, a.f00_A + base_cell * np, b, rowfull + rb);
                     } else {
                         const int np_row = 1 + 2 * min(t, a.m0);
@@ -672,7 +674,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                         for (int kk = 0; kk < np_row; ++kk) {
                             const long long off = (q0 + kk) * a.pstride + base_cell * np;
                             const size_t d = (size_t)kk * tx * np * sizeof(TS);
-                            bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
+                            if (need_Y0) bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
                             if (need_A) bulk_g2s(base + P.row_arr_bytes + d, a.pl_A + off, b, rowfull + rb);
                         }
                         q0 += np_row;
