@@ -15,9 +15,14 @@ cudaError_t batch_mc(const StageArgs<TS>& a1, const BatchWork& bw, int nc, cudaS
     // instantiation covers 257-384 threads; with m0 <= 1 a 320-thread CTA is
     // compiled for two per SM (102 registers)
     cudaError_t e = cudaErrorNotSupported;
-    if (threads <= 256) e = launch_pipe<MC, TS, 256, true>(a1, bw, threads, P.total, bw.nitems, s);
-    else if (MC <= 1 && threads <= 320) e = launch_pipe<MC, TS, 320, true>(a1, bw, threads, P.total, bw.nitems, s);
-    else if (threads <= 384) e = launch_pipe<MC, TS, 384, true>(a1, bw, threads, P.total, bw.nitems, s);
+    if (threads <= 256) {
+        e = launch_pipe<MC, TS, 256>(a1, bw, threads, P.total, bw.nitems, s);
+    } else if constexpr (MC <= 1) {
+        if (threads <= 320) e = launch_pipe<MC, TS, 320>(a1, bw, threads, P.total, bw.nitems, s);
+        else if (threads <= 384) e = launch_pipe<MC, TS, 384>(a1, bw, threads, P.total, bw.nitems, s);
+    } else if (threads <= 384) {
+        e = launch_pipe<MC, TS, 384>(a1, bw, threads, P.total, bw.nitems, s);
+    }
     if (e != cudaSuccess) return e;
     // E and B of every problem from the stage's current partial sums
     stage_fields_batch_kernel<TS><<<dim3((unsigned)bw.nprobs), dim3(128), 0, s>>>(bw.probs, bw.desc_bytes);

@@ -4,8 +4,8 @@
 // (OSHUN-1/def-RK.cpp:110-145).
 //
 // Two kernels share the helpers of this header: rk_stage_tile_kernel
-// (stage_pipe.cu) for one problem, and rk_stage_pipe_kernel<..., BATCH = true>
-// (below, launched from stage_batch.cu) for a batch of problems, whose tiles
+// (stage_pipe.cu) for one problem, and rk_stage_pipe_kernel (below, launched
+// from stage_batch.cu) for a batch of problems, whose tiles
 // carry their problem's descriptor in the header of their first copy.
 //
 // One resident CTA per SM walks tiles of `tx` consecutive cells of one y row
@@ -516,46 +516,30 @@ __host__ __device__ inline SmemPlan smem_plan(bool batch, int hdr_bytes, int nco
 // accumulators are few (m0 <= 1, the 1D batches) and the CTA has at most
 // 10 warps, so that one CTA's tile start and end latencies overlap the
 // other's work (two 12-warp CTAs would leave 80 registers a thread)
-template <int MC, int MAXT, bool BATCH>
-constexpr int batch_min_blocks() { return (BATCH && MC <= 1 && MAXT <= 320) ? 2 : 1; }
+template <int MC, int MAXT>
+constexpr int batch_min_blocks() { return (MC <= 1 && MAXT <= 320) ? 2 : 1; }
 
-template <int MC, typename TS, int MAXT, bool BATCH>
-__global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
+// a1: the launch's kernel parameter (its error word receives pipeline
+// timeouts); every item's own descriptor arrives with its first slot
+template <int MC, typename TS, int MAXT>
+__global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
     rk_stage_pipe_kernel(const StageArgs<TS> a1, const BatchWork bw) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int tid = threadIdx.x;
     const int nc = (int)blockDim.x - 64;               // consumer threads
     const int ncw = nc >> 5;                           // consumer warps
-    SmemPlan P;
-    int ntiles1 = 0;
-    if constexpr (BATCH) {
-        P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth);
-    } else {
-        const int ncoef = (a1.l0 + 1) * (a1.m0 + 1);
-        const int tx = tile_cells(a1.np, a1.nx, nc, bw.tx_cap);
-        const PipeLayout L = pipe_layout(ncoef, tx, a1.np, a1.ny > 1, (int)sizeof(TS), a1.m0);
-        P = smem_plan<TS>(false, 0, ncoef, L.slot_bytes, L.row_arr_bytes);
-        ntiles1 = a1.ny * ((a1.nx + tx - 1) / tx);
-    }
-    const int nitems = BATCH ? bw.nitems : ntiles1;
+    const SmemPlan P = smem_plan<TS>(true, bw.hdr_bytes, 0, bw.slot_bytes, bw.row_arr_bytes, bw.row_depth);
+    const int nitems = bw.nitems;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem);
     uint64_t* empty = full + kDepth;
     uint64_t* rowfull = empty + kDepth;
     uint64_t* rowempty = rowfull + kRowMax;
     // staged-row ring depth: a batch of few harmonics per row needs rows further ahead
-    const int RD = BATCH ? bw.row_depth : 2;
+    const int RD = bw.row_depth;
     unsigned char* slots = smem + P.off_slots;
     unsigned char* rows = smem + P.off_rows;
 
-    // single problem: coupling table (arithmetic type) and plane map once; barriers
-    if constexpr (!BATCH) {
-        const int ncoef = (a1.l0 + 1) * (a1.m0 + 1);
-        const double* src = reinterpret_cast<const double*>(a1.coef);
-        TS* dst = reinterpret_cast<TS*>(smem + P.off_coef);
-        for (int i = tid; i < ncoef * 16; i += blockDim.x) dst[i] = (TS)src[i];
-        int* pl = reinterpret_cast<int*>(smem + P.off_plane);
-        for (int i = tid; i < ncoef; i += blockDim.x) pl[i] = a1.plane_of[i];
-    }
+    // barriers
     if (tid == 0) {
         for (int k = 0; k < kDepth; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
         for (int k = 0; k < RD; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
@@ -563,11 +547,10 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
     }
     __syncthreads();
 
-    auto item_pid = [&](int it) -> int { return BATCH ? bw.items[it].x : 0; };
-    auto item_tile = [&](int it) -> int { return BATCH ? bw.items[it].y : it; };
+    auto item_pid = [&](int it) -> int { return bw.items[it].x; };
+    auto item_tile = [&](int it) -> int { return bw.items[it].y; };
     auto load_desc = [&](int pid) -> StageArgs<TS> {
-        if constexpr (BATCH) return *reinterpret_cast<const StageArgs<TS>*>(bw.probs + (size_t)pid * bw.desc_bytes);
-        else return a1;
+        return *reinterpret_cast<const StageArgs<TS>*>(bw.probs + (size_t)pid * bw.desc_bytes);
     };
 
     // ---------------- producer warps ----------------------------------------
@@ -624,9 +607,9 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
                         }
                         const uint32_t bpc = (uint32_t)np * esz;   // bytes per cell
                         uint32_t bytes = ncomp * ncell * bpc;
-                        if (BATCH && first) bytes += (uint32_t)bw.desc_bytes;
+                        if (first) bytes += (uint32_t)bw.desc_bytes;
                         mbar_expect_tx(full + slot, bytes);
-                        if (BATCH && first)
+                        if (first)
                             bulk_g2s(sbase, bw.probs + (size_t)pid * bw.desc_bytes, (uint32_t)bw.desc_bytes,
                                      full + slot);
                         first = false;
@@ -880,21 +863,16 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT, BATCH>())
         // the item's first slot (f00) carries the batch header; every consumer
         // warp keeps its own copy, so no barrier joins the warps
         acquire();
-        if constexpr (BATCH) {
-            unsigned char* cur = smem + P.off_cur + (size_t)(tid >> 5) * P.hdr;
-            if (!dead) {
-                const float4* s4 = reinterpret_cast<const float4*>(slots + (size_t)slot * P.slot_stride);
-                float4* d4 = reinterpret_cast<float4*>(cur);
-                for (int i = lane; i < (int)(P.hdr / 16); i += 32) d4[i] = s4[i];
-            }
-            __syncwarp();
-            // the coupling table and the plane map stay in global memory (L1-resident)
-            const StageArgs<TS>& ab = *reinterpret_cast<const StageArgs<TS>*>(cur);
-            item(ab, reinterpret_cast<const CoefT<TS>*>(ab.coef_ts), ab.plane_of, tile);
-        } else {
-            item(a1, reinterpret_cast<const CoefT<TS>*>(smem + P.off_coef),
-                 reinterpret_cast<const int*>(smem + P.off_plane), tile);
+        unsigned char* cur = smem + P.off_cur + (size_t)(tid >> 5) * P.hdr;
+        if (!dead) {
+            const float4* s4 = reinterpret_cast<const float4*>(slots + (size_t)slot * P.slot_stride);
+            float4* d4 = reinterpret_cast<float4*>(cur);
+            for (int i = lane; i < (int)(P.hdr / 16); i += 32) d4[i] = s4[i];
         }
+        __syncwarp();
+        // the coupling table and the plane map stay in global memory (L1-resident)
+        const StageArgs<TS>& ab = *reinterpret_cast<const StageArgs<TS>*>(cur);
+        item(ab, reinterpret_cast<const CoefT<TS>*>(ab.coef_ts), ab.plane_of, tile);
         if (dead) break;
     }
 }
@@ -911,12 +889,12 @@ int sm_count() {
     return n[dev];
 }
 
-template <int MC, typename TS, int MAXT, bool BATCH>
+template <int MC, typename TS, int MAXT>
 cudaError_t launch_pipe(const StageArgs<TS>& a, const BatchWork& bw, int threads, size_t smem, long long nitems,
                         cudaStream_t s) {
     static size_t attr = 0;
     if (smem > attr) {
-        cudaError_t e = cudaFuncSetAttribute(rk_stage_pipe_kernel<MC, TS, MAXT, BATCH>,
+        cudaError_t e = cudaFuncSetAttribute(rk_stage_pipe_kernel<MC, TS, MAXT>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr = smem;
@@ -924,15 +902,15 @@ cudaError_t launch_pipe(const StageArgs<TS>& a, const BatchWork& bw, int threads
     // persistent CTAs, as many as are resident at once, each walking items
     // blockIdx.x + k gridDim.x
     int per_sm = 1;
-    if (BATCH) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rk_stage_pipe_kernel<MC, TS, MAXT, BATCH>,
+    {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rk_stage_pipe_kernel<MC, TS, MAXT>,
                                                                       threads, smem);
         if (e != cudaSuccess || per_sm < 1) per_sm = 1;
     }
     const long long cap = (long long)per_sm * sm_count();
     const long long blocks = nitems < cap ? nitems : cap;
     if (blocks < 1) return cudaSuccess;
-    rk_stage_pipe_kernel<MC, TS, MAXT, BATCH><<<dim3((unsigned)blocks), dim3(threads), smem, s>>>(a, bw);
+    rk_stage_pipe_kernel<MC, TS, MAXT><<<dim3((unsigned)blocks), dim3(threads), smem, s>>>(a, bw);
     return cudaGetLastError();
 }
 
