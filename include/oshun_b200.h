@@ -47,7 +47,8 @@ typedef enum oshun_precision {
 
 /* flags */
 #define OSHUN_FLAG_FIX_YADV_CHAIN 0x1  /* drop the reference's y-advection coefficient
-                                          factor for m >= 2 (see DESIGN of the RHS) */
+                                          factor C1[l-1]/C1[m+1] that OSHUN-1 carries for
+                                          m >= 2 (def-VlasovMax.cpp:916-946) */
 
 /* Run configuration: the input-deck fields the hot path reads
  * (OSHUN-1/decl-input.h:59-138, derived values as in
@@ -131,11 +132,13 @@ int oshun_step(oshun_handle h, int nsteps, int collisions);
 int oshun_time(oshun_handle h, double* t);
 /* Status word: bit 0 = a Gauss-Seidel solve found its matrix not diagonally
  * dominant and kept f (the reference's WARNING, def-FokkerPlanck.cpp:1027-1030);
- * bit 1 = NaN/Inf in the state.  *count = skipped solves since the last call.
- * Reading clears the word. */
+ * bit 1 = NaN/Inf in the state (checked by this call); bit 4 = a pipeline wait
+ * of a stage launch gave up (that launch returned without finishing: the state
+ * is undefined).  *count = skipped solves since the last call.  Reading clears
+ * the word. */
 int oshun_status_flags(oshun_handle h, int* flags, long long* count);
 /* Device pointers of the state planes for zero-copy use: the f00 plane
- * (FP64, [numy][numx][nump]), the other planes (see oshun_plane_layout), the
+ * (FP64, [numy][numx][nump]), the other planes (see oshun_plane_index), the
  * 6 field planes; sizes in bytes. */
 int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields,
                        size_t* planes_bytes, size_t* fields_bytes);
@@ -223,14 +226,31 @@ int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, 
  *              oshun_device_state / oshun_plane_index, FP64 (read/written)
  *   Dt         implicit step (Euler_Backward's t_new - t)
  *   stream     cudaStream_t (NULL: the default stream)
- *   nondominant  optional: when not NULL the call waits for the stream and
- *              stores the number of Gauss-Seidel solves skipped as not
- *              diagonally dominant
+ *   nondominant  optional out: the number of Gauss-Seidel solves skipped as
+ *              not diagonally dominant
+ *   flags      optional out: the status word of oshun_status_flags (bit 0 =
+ *              a skipped solve, bit 1 = NaN/Inf in the result planes)
+ * Without nondominant and flags the call only enqueues work on the stream.
+ * With either, it also checks the result planes for NaN/Inf, waits for the
+ * stream, stores the outputs and returns OSHUN_ERR_NUMERIC when bit 1 is set.
  * The first call on a device looks up the array's device address; make it
  * before any stream capture.  Every call shares the array and it keeps the
  * last call's contents: calls that overlap on the GPU race on it. */
 int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, double* planes, double Dt, void* stream,
-                              long long* nondominant);
+                              long long* nondominant, int* flags);
+
+/* ---- fault injection for tests -------------------------------------------- */
+
+/* No counterpart in the reference.  Arms a failure of the pipelined stage
+ * kernel for the next oshun_rk4_step only (the captured step graphs of
+ * oshun_step never carry it): in each of that step's four stage launches the
+ * first CTA's source producer stops before its withhold_copy-th bulk copy, so
+ * the consumers waiting for that copy give up after wait_seconds (1e-4 to 1)
+ * instead of the default 1 s.  The launches return, bit 4 of the status word
+ * is set (oshun_status_flags) and the state is undefined until the next
+ * oshun_upload; the handle stays usable.  No GPU fault is involved: every
+ * wait of the kernel is bounded and every copy issued is waited for. */
+int oshun_debug_inject_stage_timeout(oshun_handle h, int withhold_copy, double wait_seconds);
 
 /* Human-readable message of the last error on this thread. */
 const char* oshun_last_error(void);

@@ -31,7 +31,7 @@ EXPORTED = [
     "oshun_batch_upload", "oshun_batch_download", "oshun_batch_step", "oshun_batch_status",
     "oshun_batch_set_tiles", "oshun_batch_get_tiles", "oshun_batch_autotune",
     "oshun_adjoint_create", "oshun_adjoint_destroy", "oshun_adjoint_set_stream", "oshun_adjoint_state_size",
-    "oshun_adjoint_forward", "oshun_adjoint_vjp",
+    "oshun_adjoint_forward", "oshun_adjoint_vjp", "oshun_debug_inject_stage_timeout",
 ]
 
 
@@ -85,8 +85,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
     lib.oshun_plane_index.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.oshun_debug_inject_stage_timeout.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     lib.oshun_collide_flm_noalloc.argtypes = [ctypes.POINTER(OshunCfg), vp, vp, ctypes.c_double, vp,
-                                              ctypes.POINTER(ctypes.c_longlong)]
+                                              ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
     ip = ctypes.POINTER(ctypes.c_int)
     if not hasattr(lib, "oshun_batch_create"):   # a build without the batch entry points
         lib.oshun_last_error.restype = ctypes.c_char_p
@@ -221,6 +222,12 @@ class Handle:
         t = ctypes.c_double()
         self._check(self.lib.oshun_time(self._h, ctypes.byref(t)), "oshun_time")
         return t.value
+
+    def inject_stage_timeout(self, withhold_copy: int, wait_seconds: float) -> None:
+        """Fault injection for tests: the next rk4_step's stage launches stop
+        one copy short and their waits give up after wait_seconds."""
+        self._check(self.lib.oshun_debug_inject_stage_timeout(self._h, withhold_copy, wait_seconds),
+                    "oshun_debug_inject_stage_timeout")
 
     def status_flags(self):
         fl = ctypes.c_int()

@@ -33,6 +33,39 @@ namespace oshun {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
+cudaError_t ensure_dyn_smem(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void*, int>, size_t>> set;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& kv : set)
+        if (kv.first.first == func && kv.first.second == dev) {
+            if (bytes <= kv.second) return cudaSuccess;
+            e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e == cudaSuccess) kv.second = bytes;
+            return e;
+        }
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) set.push_back({{func, dev}, bytes});
+    return e;
+}
+
+int sm_count() {
+    static std::mutex mu;
+    static int n[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> lk(mu);
+    if (n[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        n[dev] = v;
+    }
+    return n[dev];
+}
+
 namespace {
 
 struct Clock {
@@ -148,6 +181,12 @@ struct oshun_ctx {
     void* pl[4] = {nullptr, nullptr, nullptr, nullptr};
     void* fld[4] = {nullptr, nullptr, nullptr, nullptr};
     int cur = 0;
+
+    // fault injection for tests (oshun_debug_inject_stage_timeout): armed for
+    // the next oshun_rk4_step, active only while that step's stages launch
+    bool inject_armed = false, inject_active = false;
+    int inject_withhold = -1;
+    unsigned long long inject_wait_ns = 1000000000ull;
 
     CoefLM* d_coef = nullptr;
     int* d_plane_of = nullptr;   // [(l0+1)*(m0+1)]
@@ -280,6 +319,8 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     a.g00_s = g00_s; a.g00_inv = g00_inv; a.g00_gr = g00_gr;
     a.idx = idx; a.idy = idy;
     a.seq = d_seq; a.nh = nh; a.err = d_status;
+    a.wait_ns = inject_active ? inject_wait_ns : 1000000000ull;
+    a.withhold = inject_active ? inject_withhold : -1;
     a.jw = d_jw;
     (void)out_set;
     return a;
@@ -750,7 +791,10 @@ int oshun_rhs(oshun_handle h, double* slope_harmonics, double* slope_fields) {
 
 int oshun_rk4_step(oshun_handle h) {
     if (!h) return OSHUN_ERR_ARG;
+    h->inject_active = h->inject_armed;
+    h->inject_armed = false;
     int rc = enqueue_rk4(h);
+    h->inject_active = false;
     if (rc) return rc;
     h->cur ^= 1;
     h->t += h->cfg.dt;
@@ -831,6 +875,18 @@ int oshun_step(oshun_handle h, int nsteps, int collisions) {
         }
     }
     CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_debug_inject_stage_timeout(oshun_handle h, int withhold_copy, double wait_seconds) {
+    if (!h) return OSHUN_ERR_ARG;
+    if (withhold_copy < 0 || !(wait_seconds >= 1e-4 && wait_seconds <= 1.0)) {
+        set_error("need withhold_copy >= 0 and 1e-4 <= wait_seconds <= 1");
+        return OSHUN_ERR_ARG;
+    }
+    h->inject_armed = true;
+    h->inject_withhold = withhold_copy;
+    h->inject_wait_ns = (unsigned long long)(wait_seconds * 1e9);
     return OSHUN_OK;
 }
 

@@ -933,11 +933,9 @@ int collide_max_chunk(int np, size_t smem_budget) {
 int collide_threads() { return kCollideThreads; }
 
 cudaError_t launch_collide(const CollideArgs& a, cudaStream_t st, size_t smem, int blocks) {
-    static size_t attr_bytes = 0;
-    if (smem > attr_bytes) {
-        cudaError_t e = cudaFuncSetAttribute(collide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_kernel, smem);
         if (e != cudaSuccess) return e;
-        attr_bytes = smem;
     }
     collide_kernel<<<blocks, kCollideThreads, smem, st>>>(a);
     return cudaGetLastError();
@@ -953,12 +951,9 @@ template <typename TP, int E>
 cudaError_t launch_lane(const CollideArgs& a, cudaStream_t st, int blocks, size_t smem) {
     // planes per batch: two row sets of P x E doubles stay in registers
     constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
-    static size_t attr = 0;
-    if (smem > attr) {
-        cudaError_t e = cudaFuncSetAttribute(collide_lane_kernel<TP, E, P>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_lane_kernel<TP, E, P>, smem);
         if (e != cudaSuccess) return e;
-        attr = smem;
     }
     collide_lane_kernel<TP, E, P><<<blocks, 32, smem, st>>>(a);
     return cudaGetLastError();
@@ -983,12 +978,9 @@ namespace {
 template <typename TP, int E>
 cudaError_t launch_lane_batch(const CollideBatch& b, cudaStream_t st, size_t smem) {
     constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
-    static size_t attr = 0;
-    if (smem > attr) {
-        cudaError_t e = cudaFuncSetAttribute(collide_lane_batch_kernel<TP, E, P>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_lane_batch_kernel<TP, E, P>, smem);
         if (e != cudaSuccess) return e;
-        attr = smem;
     }
     const long long blocks = b.nitems < (1ll << 30) ? b.nitems : (1ll << 30);
     if (blocks < 1) return cudaSuccess;
@@ -1029,12 +1021,9 @@ template <typename TP, int E>
 cudaError_t launch_lane_chunk(const CollideBatch& b, cudaStream_t st) {
     constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
     const size_t smem = collide_chunk_smem(b.warps, b.tab_doubles, b.cell_doubles);
-    static size_t attr = 0;
-    if (smem > attr) {
-        cudaError_t e = cudaFuncSetAttribute(collide_lane_chunk_kernel<TP, E, P>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_lane_chunk_kernel<TP, E, P>, smem);
         if (e != cudaSuccess) return e;
-        attr = smem;
     }
     const long long blocks = b.nchunks < (1ll << 30) ? b.nchunks : (1ll << 30);
     if (blocks < 1) return cudaSuccess;
@@ -1103,22 +1092,13 @@ cudaError_t launch_collide_tri(const CollideArgs& a, cudaStream_t st, int /*cell
         if (a.planes_fp32) return launch_lane_e<float>(a, st, blocks, smem);
         return launch_lane_e<double>(a, st, blocks, smem);
     }
-    static size_t attr64 = 0, attr32 = 0;
     if (a.planes_fp32) {
-        if (smem > attr32) {
-            cudaError_t e = cudaFuncSetAttribute(collide_warp_kernel<float>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr32 = smem;
-        }
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_warp_kernel<float>, smem);
+        if (e != cudaSuccess) return e;
         collide_warp_kernel<float><<<blocks, 32, smem, st>>>(a);
     } else {
-        if (smem > attr64) {
-            cudaError_t e = cudaFuncSetAttribute(collide_warp_kernel<double>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr64 = smem;
-        }
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_warp_kernel<double>, smem);
+        if (e != cudaSuccess) return e;
         collide_warp_kernel<double><<<blocks, 32, smem, st>>>(a);
     }
     return cudaGetLastError();

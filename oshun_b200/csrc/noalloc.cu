@@ -12,7 +12,9 @@
 //
 // The kernel is the collision kernel of collide.cu (launch_collide), the
 // staged-chunk / dense Gauss-Seidel variant, run with do_ee = 0 and both f1
-// and f_lm steps; only the source of its scratch differs.
+// and f_lm steps; only the source of its scratch differs.  A small kernel
+// writes the velocity tables and plane maps into the array first, so the
+// call stages nothing in host memory.
 //
 // Set-up: the first call on a device, with that device current, looks up
 // the device address of the array (cudaGetSymbolAddress) and caches it; make
@@ -32,7 +34,6 @@ namespace {
 constexpr size_t kScratchBytes = 32ull << 20;   // 32 MiB
 constexpr int kMaxDevices = 64;
 constexpr int kMaxL0 = 64;
-constexpr int kMaxCoef = (kMaxL0 + 1) * (kMaxM0 + 1);
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -47,9 +48,66 @@ size_t off_dense(int np, int ncoef, int nplanes) {
     return off_ints(np) + (((size_t)ncoef + 2 * (size_t)nplanes) * sizeof(int) + 255) / 256 * 256;
 }
 
-double axis_point(int i, int n, double lo, double hi) {
-    const double step = (hi - lo) / (double)(n - 1);
-    return (double)i * step + lo;
+// The velocity-grid tables of the collision operators
+// (OSHUN-1/def-FokkerPlanck.cpp:143-172, 790-803) and the plane maps, built
+// on the device straight into the scratch array, so the call keeps no host
+// staging buffer alive after it returns.  The arithmetic mirrors the handle's
+// host-side tables operation by operation (no contracted multiply-adds).
+__global__ void __launch_bounds__(256) noalloc_tables_kernel(double* V, int* plane_of, int* plane_l, int* plane_m,
+                                                             int* status, int np, int l0, int m0, double pmin,
+                                                             double pmax) {
+    const int t = threadIdx.x;
+    if (t < 4) status[t] = 0;   // the status word starts at zero every call
+    const double step = __ddiv_rn(__dsub_rn(pmax, pmin), (double)(np - 1));
+    double* vr = V;
+    for (int i = t; i < np; i += blockDim.x) {
+        const double p = __dadd_rn(__dmul_rn((double)i, step), pmin);
+        vr[i] = __ddiv_rn(p, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(p, p))));
+    }
+    __syncthreads();
+    for (int i = t; i < np; i += blockDim.x) {
+        const double v = vr[i];
+        if (i >= 1) {
+            const double w = vr[i - 1];
+            const double dv = __dsub_rn(v, w);
+            V[np + i] = __dmul_rn(__dmul_rn(0.5, pow(v, 4.0)), dv);
+            V[2 * np + i] = __dmul_rn(__dmul_rn(0.5, pow(w, 4.0)), dv);
+            V[3 * np + i] = __dmul_rn(__dmul_rn(__dmul_rn(0.5, v), v), dv);
+            V[4 * np + i] = __dmul_rn(__dmul_rn(__dmul_rn(0.5, w), w), dv);
+            V[5 * np + i] = __dmul_rn(__dmul_rn(0.5, v), dv);
+            V[6 * np + i] = __dmul_rn(__dmul_rn(0.5, w), dv);
+        } else {
+            for (int k = 1; k <= 6; ++k) V[k * np] = 0.0;
+        }
+        V[7 * np + i] = pow(v, 3.0);
+        V[10 * np + i] = pow(v, 5.0);
+        V[11 * np + i] = pow(v, 7.0);
+        if (i == 0)
+            V[8 * np] = __ddiv_rn(1.0, __ddiv_rn(__dmul_rn(__dmul_rn(vr[0], vr[0]), vr[1]), 2.0));
+        else if (i < np - 1)
+            V[8 * np + i] = __ddiv_rn(1.0, __ddiv_rn(__dmul_rn(__dmul_rn(v, v), __dsub_rn(vr[i + 1], vr[i - 1])), 2.0));
+        else
+            V[8 * np + i] = 0.0;
+        if (i < np - 1)
+            V[9 * np + i] = __ddiv_rn(1.0, __dmul_rn(__ddiv_rn(__dsub_rn(vr[i + 1], v), 2.0), __dadd_rn(vr[i + 1], v)));
+        else
+            V[9 * np + i] = 0.0;
+    }
+    // plane maps (the handle's plane order: l >= 1, m <= min(l, m0), Re then Im)
+    if (t == 0) {
+        const int ncoef = (l0 + 1) * (m0 + 1);
+        for (int i = 0; i < ncoef; ++i) plane_of[i] = -1;
+        int q = 0;
+        for (int l = 1; l <= l0; ++l)
+            for (int m = 0; m <= (l < m0 ? l : m0); ++m) {
+                plane_of[l * (m0 + 1) + m] = q;
+                for (int k = 0; k < (m > 0 ? 2 : 1); ++k) {
+                    plane_l[q] = l;
+                    plane_m[q] = m;
+                    ++q;
+                }
+            }
+    }
 }
 
 }  // namespace
@@ -58,7 +116,7 @@ double axis_point(int i, int n, double lo, double hi) {
 using namespace oshun;
 
 extern "C" int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, double* planes, double Dt,
-                                         void* stream, long long* nondominant) {
+                                         void* stream, long long* nondominant, int* flags) {
     if (!cfg || !f00 || !planes) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
     const oshun_cfg& c = *cfg;
     if (c.precision != OSHUN_FP64) { set_error("noalloc collision step: FP64 planes only"); return OSHUN_ERR_UNSUPPORTED; }
@@ -74,21 +132,9 @@ extern "C" int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, doub
     const int np = c.nump, l0 = c.l0, m0 = c.m0;
     const long long cells = (long long)c.numx * c.numy;
     const int ncoef = (l0 + 1) * (m0 + 1);
-
-    // plane maps (the handle's plane order: l >= 1, m <= min(l, m0), Re then Im)
-    int plane_of[kMaxCoef];
-    int plane_lm[2 * 2 * kMaxCoef];
     int nplanes = 0;
-    for (int i = 0; i < ncoef; ++i) plane_of[i] = -1;
     for (int l = 1; l <= l0; ++l)
-        for (int m = 0; m <= (l < m0 ? l : m0); ++m) {
-            plane_of[l * (m0 + 1) + m] = nplanes;
-            for (int k = 0; k < (m > 0 ? 2 : 1); ++k) {
-                plane_lm[nplanes] = l;
-                plane_lm[2 * kMaxCoef + nplanes] = m;
-                ++nplanes;
-            }
-        }
+        for (int m = 0; m <= (l < m0 ? l : m0); ++m) nplanes += m > 0 ? 2 : 1;
 
     // size check against the fixed scratch
     int dev = 0;
@@ -139,35 +185,6 @@ extern "C" int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, doub
     unsigned char* sb = static_cast<unsigned char*>(base);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-    // velocity-grid tables of the collision operators
-    // (OSHUN-1/def-FokkerPlanck.cpp:143-172, 790-803)
-    double V[12 * kMaxNp];
-    std::memset(V, 0, sizeof(double) * 12 * np);
-    double* vr = V;
-    for (int i = 0; i < np; ++i) {
-        const double p = axis_point(i, np, c.pmin, c.pmax);
-        vr[i] = p / std::sqrt(1.0 + p * p);
-    }
-    for (int i = 1; i < np; ++i) {
-        const double dv = vr[i] - vr[i - 1];
-        V[np + i] = 0.5 * std::pow(vr[i], 4) * dv;
-        V[2 * np + i] = 0.5 * std::pow(vr[i - 1], 4) * dv;
-        V[3 * np + i] = 0.5 * vr[i] * vr[i] * dv;
-        V[4 * np + i] = 0.5 * vr[i - 1] * vr[i - 1] * dv;
-        V[5 * np + i] = 0.5 * vr[i] * dv;
-        V[6 * np + i] = 0.5 * vr[i - 1] * dv;
-    }
-    for (int i = 0; i < np; ++i) {
-        V[7 * np + i] = std::pow(vr[i], 3);
-        V[10 * np + i] = std::pow(vr[i], 5);
-        V[11 * np + i] = std::pow(vr[i], 7);
-    }
-    V[8 * np] = 1.0 / ((vr[0] * vr[0] * vr[1]) / 2.0);
-    for (int i = 1; i < np - 1; ++i) V[8 * np + i] = 1.0 / (vr[i] * vr[i] * (vr[i + 1] - vr[i - 1]) / 2.0);
-    for (int i = 0; i < np - 1; ++i) V[9 * np + i] = 1.0 / ((vr[i + 1] - vr[i]) / 2.0 * (vr[i + 1] + vr[i]));
-    const double kRe = 2.8179402894e-13;
-    const double kp = std::sqrt(4.0 * M_PI * c.density_np * kRe);
-
     double* dV = reinterpret_cast<double*>(sb + kOffTables);
     int* dI = reinterpret_cast<int*>(sb + off_ints(np));
     int* dstatus = reinterpret_cast<int*>(sb + kOffStatus);
@@ -179,12 +196,11 @@ extern "C" int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, doub
             return OSHUN_ERR_CUDA;                                                            \
         }                                                                                     \
     } while (0)
-    // the host tables are on this thread's stack: copy synchronously before returning
-    CKN(cudaMemcpyAsync(dV, V, sizeof(double) * 12 * np, cudaMemcpyHostToDevice, st));
-    CKN(cudaMemcpyAsync(dI, plane_of, sizeof(int) * ncoef, cudaMemcpyHostToDevice, st));
-    CKN(cudaMemcpyAsync(dI + ncoef, plane_lm, sizeof(int) * nplanes, cudaMemcpyHostToDevice, st));
-    CKN(cudaMemcpyAsync(dI + ncoef + nplanes, plane_lm + 2 * kMaxCoef, sizeof(int) * nplanes, cudaMemcpyHostToDevice, st));
-    CKN(cudaMemsetAsync(dstatus, 0, 4 * sizeof(int), st));   // the status word starts at zero every call
+    noalloc_tables_kernel<<<1, 256, 0, st>>>(dV, dI, dI + ncoef, dI + ncoef + nplanes, dstatus, np, l0, m0, c.pmin,
+                                             c.pmax);
+    CKN(cudaGetLastError());
+    const double kRe = 2.8179402894e-13;
+    const double kp = std::sqrt(4.0 * M_PI * c.density_np * kRe);
 
     CollideArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -210,11 +226,19 @@ extern "C" int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, doub
     a.dense_ws = c.if_tridiagonal ? nullptr : reinterpret_cast<double*>(sb + dense_off);
     a.status = dstatus;
     CKN(launch_collide(a, st, smem, blocks));
-    if (nondominant) {
+    if (nondominant || flags) {
+        // NaN/Inf in the result planes sets bit 1; then wait for the stream
+        // and report the status word
+        CKN(launch_nan_check(f00, planes, 0, cells * np, (long long)nplanes * cells * np, nullptr, 0, dstatus, st));
         int h_status[2] = {0, 0};
         CKN(cudaMemcpyAsync(h_status, dstatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
         CKN(cudaStreamSynchronize(st));
-        *nondominant = h_status[1];
+        if (nondominant) *nondominant = h_status[1];
+        if (flags) *flags = h_status[0];
+        if (h_status[0] & 2) {
+            set_error("noalloc collision step: NaN/Inf in the result planes");
+            return OSHUN_ERR_NUMERIC;
+        }
     }
 #undef CKN
     return OSHUN_OK;

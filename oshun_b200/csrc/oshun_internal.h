@@ -61,6 +61,8 @@ struct StageArgs {
     const int* seq;       // [nh]: source harmonics in stream order, s | (m << 16)
     int nh;
     int* err;             // error word (bit 4: a pipeline wait timed out)
+    unsigned long long wait_ns;   // a pipeline wait gives up after this many ns (single-problem kernel)
+    int withhold;         // fault injection for tests: CTA 0's source producer skips this copy (-1: none)
     const void* coef_ts;  // coupling table in the arithmetic type (batched launches)
     double* jw;           // [cells][3][8]: per-warp partial sums of Jx, Re Jy, Im Jy (single-problem pipeline)
 };
@@ -163,5 +165,12 @@ cudaError_t launch_nan_check(const double* f00, const void* planes, int planes_f
                              cudaStream_t s);
 
 void set_error(const std::string& msg);
+
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
+// device.  The attribute is per device, so the size already set is cached
+// per (kernel, device), under a lock (launchers may run on several threads).
+cudaError_t ensure_dyn_smem(const void* func, size_t bytes);
+// SM count of the current device (148 when the query fails)
+int sm_count();
 
 }  // namespace oshun

@@ -36,6 +36,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     const bool need_Y0 = need_B && (a.first || a.f00_out != nullptr);
 
     const int tid = threadIdx.x;
+    const unsigned long long wlim = a.wait_ns;   // every pipeline wait gives up after this
     const int tiles_x = (nx + tx - 1) / tx;
     const int ntiles = tiles_x * ny;
     // persistent CTAs: tiles blockIdx.x, blockIdx.x + gridDim.x, ...
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         if (tid == nct) {
             // source warp: every harmonic of the stage input, (l, m) order, tile after tile
             int issued = 0;
-            bool ok = true;
+            bool ok = true, injected = false;
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 const int y = tile / tiles_x;
                 const int x0 = (tile - y * tiles_x) * tx;
@@ -77,7 +78,14 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 for (int s = 0; s <= a.l0 && ok; ++s) {
                     for (int m = 0; m <= min(s, a.m0); ++m) {
                         const int slot = issued % D, j = issued / D;
-                        if (j >= 1 && !mbar_wait(empty + slot, (uint32_t)((j - 1) & 1))) { ok = false; break; }
+                        if (issued == a.withhold && blockIdx.x == 0) {
+                            // fault injection (tests): this copy and every later one is
+                            // withheld, so the consumers' waits for it run out
+                            injected = true;
+                            ok = false;
+                            break;
+                        }
+                        if (j >= 1 && !mbar_wait(empty + slot, (uint32_t)((j - 1) & 1), wlim)) { ok = false; break; }
                         unsigned char* dst = slots + (size_t)slot * L.slot_bytes;
                         const unsigned char* src;
                         int esz, ncomp;
@@ -113,10 +121,10 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 }
             }
             if (!ok) {
-                atomicOr(a.err, 16);
+                if (!injected) atomicOr(a.err, 16);
                 // bounded drain of every copy that may still be in flight
                 for (int idx = max(0, issued - D); idx < issued; ++idx)
-                    mbar_wait(full + (idx % D), (uint32_t)((idx / D) & 1));
+                    mbar_wait(full + (idx % D), (uint32_t)((idx / D) & 1), wlim);
             }
         } else if (tid == nct + 32 && need_B) {
             // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
@@ -130,7 +138,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 const long long base_cell = (long long)y * nx + x0;
                 for (int t = 0; t <= a.l0; ++t) {
                     const int rb = issued & 1, k = issued >> 1;
-                    if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1))) { ok = false; break; }
+                    if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1), wlim)) { ok = false; break; }
                     unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
                     const uint32_t nb = (need_Y0 ? 1 : 0) + (need_A ? 1 : 0);
                     if (t == 0) {
@@ -162,7 +170,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
             if (!ok) {
                 atomicOr(a.err, 16);
                 for (int t = max(0, issued - 2); t < issued; ++t)
-                    mbar_wait(rowfull + (t & 1), (uint32_t)((t >> 1) & 1));
+                    mbar_wait(rowfull + (t & 1), (uint32_t)((t >> 1) & 1), wlim);
             }
         }
         return;
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     int tile_iter = 0;
 
     auto acquire = [&]() {
-        if (!dead && !mbar_wait(full + slot, phase)) {
+        if (!dead && !mbar_wait(full + slot, phase, wlim)) {
             atomicOr(a.err, 16);
             dead = true;
         }
@@ -222,7 +230,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         if (need_B) {
             // the row warp staged this tile's fields with its row 0
             const int rb = rows_used & 1;
-            if (!dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
+            if (!dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1), wlim)) {
                 atomicOr(a.err, 16);
                 dead = true;
             }
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         // RK epilogue of target row t (slopes Rt, It) from the staged Y0/Y rows
         auto epilogue = [&](const int t, const Acc<TS, MC>& At) {
             const int rb = rows_used & 1;
-            if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1))) {
+            if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1), wlim)) {
                 atomicOr(a.err, 16);
                 dead = true;
             }
@@ -369,12 +377,9 @@ __global__ void __launch_bounds__(256) stage_fields_kernel(const StageArgs<TS> a
 
 template <int MC, typename TS, int MAXT>
 cudaError_t launch_tile(const StageArgs<TS>& a, int tx, const PipeLayout& L, cudaStream_t s) {
-    static size_t attr = 0;
-    if (L.total > attr) {
-        cudaError_t e = cudaFuncSetAttribute(rk_stage_tile_kernel<MC, TS, MAXT>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)rk_stage_tile_kernel<MC, TS, MAXT>, L.total);
         if (e != cudaSuccess) return e;
-        attr = L.total;
     }
     const int np_pad = ((a.np + 31) / 32) * 32;
     const long long tiles = (long long)a.ny * ((a.nx + tx - 1) / tx);

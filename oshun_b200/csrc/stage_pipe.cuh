@@ -94,14 +94,15 @@ __device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
         : "memory");
     return done != 0;
 }
-// bounded wait for the phase with this parity; false after kWaitNs
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// bounded wait for the phase with this parity; false after limit_ns
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          const unsigned long long limit_ns = kWaitNs) {
     const uint32_t addr = smem_u32(bar);
     if (mbar_try(addr, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (;;) {
         if (mbar_try(addr, parity)) return true;
-        if (global_ns() - t0 > kWaitNs) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 // global -> shared bulk copy completing on `bar`; 16-byte aligned, size % 16 == 0
@@ -861,10 +862,13 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int tile = item_tile(it);
         // the item's first slot (f00) carries the batch header; every consumer
-        // warp keeps its own copy, so no barrier joins the warps
+        // warp keeps its own copy, so no barrier joins the warps.  A wait
+        // that ran out here leaves no descriptor to read: the warp stops
+        // before item() touches any descriptor field.
         acquire();
+        if (dead) break;
         unsigned char* cur = smem + P.off_cur + (size_t)(tid >> 5) * P.hdr;
-        if (!dead) {
+        {
             const float4* s4 = reinterpret_cast<const float4*>(slots + (size_t)slot * P.slot_stride);
             float4* d4 = reinterpret_cast<float4*>(cur);
             for (int i = lane; i < (int)(P.hdr / 16); i += 32) d4[i] = s4[i];
@@ -877,27 +881,12 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
     }
 }
 
-int sm_count() {
-    static int n[64] = {0};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (n[dev] == 0) {
-        int v = 0;
-        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
-        n[dev] = v;
-    }
-    return n[dev];
-}
-
 template <int MC, typename TS, int MAXT>
 cudaError_t launch_pipe(const StageArgs<TS>& a, const BatchWork& bw, int threads, size_t smem, long long nitems,
                         cudaStream_t s) {
-    static size_t attr = 0;
-    if (smem > attr) {
-        cudaError_t e = cudaFuncSetAttribute(rk_stage_pipe_kernel<MC, TS, MAXT>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)rk_stage_pipe_kernel<MC, TS, MAXT>, smem);
         if (e != cudaSuccess) return e;
-        attr = smem;
     }
     // persistent CTAs, as many as are resident at once, each walking items
     // blockIdx.x + k gridDim.x

@@ -61,3 +61,28 @@ def test_reference_yadv_chain_factor_is_real(oracle):
     finally:
         oracle.set_yadv_chain(True)
     assert err > 1e-3
+
+
+def nondominant_case():
+    """A dense-mode deck whose l = 3 matrices fail the reference's dominance
+    test in every cell (f00 negated, so the scattering term turns the diagonal
+    negative): Gauss_Seidel returns false and the solve keeps f
+    (OSHUN-1/def-Nmethods.cpp:70-76, def-FokkerPlanck.cpp:1021-1032)."""
+    d = Deck(l0=3, m0=2, nump=24, numx=4, numy=1, if_implicit1D=1, if_tridiagonal=0, dt=5.0, small_dt=5.0,
+             density_np=1e21, xmax=2.0)
+    st = _zero_m(seeded_state(d, seed=5, fields=False))
+    st.f[0] *= -1.0
+    return st
+
+
+def test_nondominant_skip_matches_reference(oracle):
+    import numpy as np
+    st = nondominant_case()
+    d = st.deck
+    ref = run_reference(st, ["step:1:12"])
+    out = oracle.steps(st, 1, 12)
+    assert oracle.nondominant() == d.numx          # one skipped solve (l = 3) per cell
+    err, where = worst_rel(out, ref)
+    assert err <= TOL, (err, where)
+    assert np.array_equal(ref.harmonic(3, 0), st.harmonic(3, 0))      # kept
+    assert not np.array_equal(ref.harmonic(2, 0), st.harmonic(2, 0))  # solved
