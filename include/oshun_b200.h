@@ -145,6 +145,50 @@ int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields,
 /* Plane index of the real part of harmonic (l,m) in `planes` (the imaginary
  * part, m > 0, follows it), or -1 for (0,0), which lives in `f00`. */
 int oshun_plane_index(oshun_handle h, int l, int m, int* plane);
+/* The configuration the handle was created with. */
+int oshun_get_config(oshun_handle h, oshun_cfg* cfg);
+
+/* ---- moments on the device -------------------------------------------------- */
+
+/* Parallel_Output::nonrelativistic_moments (OSHUN-1/def-Parallel.cpp:1677-2258)
+ * for every cell, computed on the device from the current state; out receives
+ * OSHUN_NUM_MOMENTS float planes [numy][numx] in the order below (the
+ * reference's Matrix2D<float> results in its normalised units; N is the
+ * density those moments divide by, 1 where it is below 4 FLT_EPSILON).  The
+ * reference's float accumulation order is kept, so results agree with its
+ * output files to a few float ulps.  Harmonics the run does not carry
+ * (f11, f2m for small l0, m0) count as zero.  Kx (Ky) needs numx (numy) >= 3;
+ * with fewer cells the derivative of <v^2>^2 is taken as zero. */
+enum oshun_moment {
+    OSHUN_MOM_N = 0, OSHUN_MOM_VX, OSHUN_MOM_VY, OSHUN_MOM_VXVX, OSHUN_MOM_VYVY, OSHUN_MOM_VZVZ,
+    OSHUN_MOM_VXVY, OSHUN_MOM_VXVZ, OSHUN_MOM_VYVZ, OSHUN_MOM_VSQ, OSHUN_MOM_T_EV, OSHUN_MOM_P_MBAR,
+    OSHUN_MOM_ND, OSHUN_MOM_NU, OSHUN_MOM_QX, OSHUN_MOM_KX, OSHUN_MOM_QY, OSHUN_MOM_KY, OSHUN_NUM_MOMENTS
+};
+int oshun_moments(oshun_handle h, float* out);
+
+/* ---- restart files ---------------------------------------------------------- */
+
+/* The reference's restart files, byte for byte (Restart_Facility::Write/Read,
+ * OSHUN-1/def-Export.cpp:733-836): <prefix>_<rank:06>_<step:03>.dat (prefix
+ * NULL = "RESTART/re", the reference's), the Stat written raw with
+ * guard_cells (the deck's RKLevel) guard cells per side: every harmonic in
+ * ind(l,m) order as complex128 [numy+2g][numx+2g][nump], then the 6 fields as
+ * complex128 [numy+2g][numx+2g].  Guards hold the periodic image of the
+ * interior, as the reference leaves them after each step
+ * (def-Parallel.cpp:1138-1158, 1229-1248); a 1D run (numy = 1) has 1 + 2g
+ * rows, each holding the interior row.  Reading takes the interior cells (and
+ * uploads them: OSHUN_ERR_NONREAL as oshun_upload).  A periodic image needs
+ * numx (and numy > 1) >= guard_cells.
+ * The pack/unpack forms convert between host buffers in the oshun_download
+ * layout and a file image; they need no device. */
+long long oshun_restart_bytes(const oshun_cfg* cfg, int guard_cells);
+int oshun_restart_pack(const oshun_cfg* cfg, int guard_cells, const double* harmonics, const double* fields,
+                       double* image);
+int oshun_restart_unpack(const oshun_cfg* cfg, int guard_cells, const double* image, double* harmonics,
+                         double* fields);
+int oshun_restart_write(oshun_handle h, const char* prefix, int rank, int re_step, int guard_cells);
+int oshun_restart_read(oshun_handle h, const char* prefix, int rank, int re_step, int guard_cells);
+
 /* ---- batches of independent problems -------------------------------------- */
 
 /* No counterpart in the reference, whose runs are one problem per process

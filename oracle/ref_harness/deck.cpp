@@ -52,6 +52,12 @@ Inputdata::input_list::input_list() {
     density_np = g_deck.density_np;
     numx = numx_glob + 2 * RKLevel;
     numy = numy_glob + 2 * RKLevel;
+    // every moment of Parallel_Output::nonrelativistic_moments on, in the
+    // reference's normalised units (def-Input.cpp:197-253, 170-172)
+    o_Vx = o_Vy = o_VxVx = o_VyVy = o_VzVz = o_VxVy = o_VxVz = o_VyVz = true;
+    o_Vsq = o_Qx = o_Qy = o_Pressure = o_Temperature = o_ND = o_Nu = true;
+    denormalize_fields = false;
+    denormalize_length = false;
 }
 
 Inputdata::decl_input::decl_input(input_list in)

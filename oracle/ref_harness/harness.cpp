@@ -16,6 +16,14 @@
 //                    MASK bit 1 rk4.advance_p1, 2 ee.loop, 4 eb.advance_1,
 //                    8 eb.advance_lm; default 15
 //   time             print the wall time of the step loops to stdout
+//   restart_write:R:S  Restart_Facility::Write(R, S, Y) (def-Export.cpp:768-800):
+//                    RESTART/re_<R>_<S>.dat in the working directory
+//   restart_read:R:S   Restart_Facility::Read(R, S, Y) (def-Export.cpp:733-766)
+//   moments:S        Parallel_Output::nonrelativistic_moments(S, Y)
+//                    (def-Parallel.cpp:1677-2258) with every moment output on:
+//                    OUTPUT/MOM/<name>/... text files in the working directory
+// The restart and moment ops also link def-Export.cpp, def-Output.cpp and
+// def-Parallel.cpp (single rank, the MPI stand-in of mpi.h here).
 //
 // Case file (little-endian), shared with oracle/oshun_oracle.c and the tests:
 //   char magic[4] = "OSHC"; int32 version = 1;
@@ -48,6 +56,12 @@
 #include "decl-RK.h"
 #include "decl-nmethods.h"
 #include "decl-fokkerplanck.h"
+#include <fstream>
+#include <sstream>
+#include <mpi.h>
+#include "decl-output.h"
+#include "decl-export.h"
+#include "decl-parallel.h"
 #include "deck.h"
 
 namespace {
@@ -260,6 +274,24 @@ int main(int argc, char** argv) {
                 refresh_guards(Y);
             }
             elapsed += now_s() - t0;
+        } else if (op.compare(0, 14, "restart_write:") == 0 || op.compare(0, 13, "restart_read:") == 0) {
+            const bool wr = op[8] == 'w';
+            int rank = 0, re_step = 0;
+            if (std::sscanf(op.c_str() + (wr ? 14 : 13), "%d:%d", &rank, &re_step) != 2) {
+                std::fprintf(stderr, "oshun_ref: bad op %s\n", op.c_str());
+                return 2;
+            }
+            Restart_Facility re;
+            if (wr) re.Write(rank, re_step, Y);
+            else re.Read(rank, re_step, Y);
+        } else if (op.compare(0, 8, "moments:") == 0) {
+            int mstep = 0;
+            if (std::sscanf(op.c_str() + 8, "%d", &mstep) != 1) {
+                std::fprintf(stderr, "oshun_ref: bad op %s\n", op.c_str());
+                return 2;
+            }
+            Parallel_Output po;
+            po.nonrelativistic_moments((size_t)mstep, Y);
         } else {
             std::fprintf(stderr, "oshun_ref: unknown op %s\n", op.c_str());
             return 2;

@@ -31,7 +31,9 @@ EXPORTED = [
     "oshun_batch_upload", "oshun_batch_download", "oshun_batch_step", "oshun_batch_status",
     "oshun_batch_set_tiles", "oshun_batch_get_tiles", "oshun_batch_autotune",
     "oshun_adjoint_create", "oshun_adjoint_destroy", "oshun_adjoint_set_stream", "oshun_adjoint_state_size",
-    "oshun_adjoint_forward", "oshun_adjoint_vjp", "oshun_debug_inject_stage_timeout",
+    "oshun_adjoint_forward", "oshun_adjoint_vjp", "oshun_debug_inject_stage_timeout", "oshun_get_config",
+    "oshun_moments", "oshun_restart_bytes", "oshun_restart_pack", "oshun_restart_unpack", "oshun_restart_write",
+    "oshun_restart_read",
 ]
 
 
@@ -86,6 +88,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
     lib.oshun_plane_index.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.oshun_debug_inject_stage_timeout.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    lib.oshun_get_config.argtypes = [vp, ctypes.POINTER(OshunCfg)]
+    lib.oshun_moments.argtypes = [vp, vp]
+    lib.oshun_restart_bytes.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int]
+    lib.oshun_restart_bytes.restype = ctypes.c_longlong
+    lib.oshun_restart_pack.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int, vp, vp, vp]
+    lib.oshun_restart_unpack.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int, vp, vp, vp]
+    lib.oshun_restart_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.oshun_restart_read.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.oshun_collide_flm_noalloc.argtypes = [ctypes.POINTER(OshunCfg), vp, vp, ctypes.c_double, vp,
                                               ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)]
     ip = ctypes.POINTER(ctypes.c_int)
@@ -229,6 +239,24 @@ class Handle:
         self._check(self.lib.oshun_debug_inject_stage_timeout(self._h, withhold_copy, wait_seconds),
                     "oshun_debug_inject_stage_timeout")
 
+    MOMENTS = ("N", "Vx", "Vy", "VxVx", "VyVy", "VzVz", "VxVy", "VxVz", "VyVz", "Vsq", "T_eV", "P_Mbar", "ND",
+               "Nu", "Qx", "Kx", "Qy", "Ky")
+
+    def moments(self) -> np.ndarray:
+        """float32 [18][numy][numx]: Parallel_Output::nonrelativistic_moments
+        of the current state, computed on the device (order: MOMENTS)."""
+        out = np.empty((len(self.MOMENTS), self.cfg.numy, self.cfg.numx), np.float32)
+        self._check(self.lib.oshun_moments(self._h, self._ptr(out)), "oshun_moments")
+        return out
+
+    def restart_write(self, prefix: str, rank: int, re_step: int, guard_cells: int = 4) -> None:
+        self._check(self.lib.oshun_restart_write(self._h, prefix.encode(), rank, re_step, guard_cells),
+                    "oshun_restart_write")
+
+    def restart_read(self, prefix: str, rank: int, re_step: int, guard_cells: int = 4) -> None:
+        self._check(self.lib.oshun_restart_read(self._h, prefix.encode(), rank, re_step, guard_cells),
+                    "oshun_restart_read")
+
     def status_flags(self):
         fl = ctypes.c_int()
         cnt = ctypes.c_longlong()
@@ -241,6 +269,39 @@ class Handle:
         self._check(self.lib.oshun_device_state(self._h, ctypes.byref(f00), ctypes.byref(pl), ctypes.byref(fl),
                                                 ctypes.byref(pb), ctypes.byref(fb)), "oshun_device_state")
         return f00.value, pl.value, fl.value, pb.value, fb.value
+
+
+def restart_pack(cfg: dict, f: np.ndarray, fields: np.ndarray, guard_cells: int = 4) -> bytes:
+    """The reference's restart-file image of a host state (no device needed)."""
+    lib = load()
+    c = make_cfg(**cfg)
+    n = lib.oshun_restart_bytes(ctypes.byref(c), guard_cells)
+    if n < 0:
+        raise OshunError(1, "oshun_restart_bytes", lib.oshun_last_error().decode())
+    img = np.empty(n // 8, np.float64)
+    f = np.ascontiguousarray(f, np.complex128)
+    fields = np.ascontiguousarray(fields, np.complex128)
+    rc = lib.oshun_restart_pack(ctypes.byref(c), guard_cells, f.ctypes.data, fields.ctypes.data, img.ctypes.data)
+    if rc:
+        raise OshunError(rc, "oshun_restart_pack", lib.oshun_last_error().decode())
+    return img.tobytes()
+
+
+def restart_unpack(cfg: dict, image: bytes, guard_cells: int = 4):
+    """Interior state (f, fields) of a restart-file image."""
+    lib = load()
+    c = make_cfg(**cfg)
+    n = lib.oshun_restart_bytes(ctypes.byref(c), guard_cells)
+    if n != len(image):
+        raise OshunError(1, "oshun_restart_unpack", f"image holds {len(image)} bytes, the configuration {n}")
+    nh = ((c.m0 + 1) * (2 * c.l0 - c.m0 + 2)) // 2
+    f = np.empty((nh, c.numy, c.numx, c.nump), np.complex128)
+    fields = np.empty((6, c.numy, c.numx), np.complex128)
+    img = np.frombuffer(image, np.float64)
+    rc = lib.oshun_restart_unpack(ctypes.byref(c), guard_cells, img.ctypes.data, f.ctypes.data, fields.ctypes.data)
+    if rc:
+        raise OshunError(rc, "oshun_restart_unpack", lib.oshun_last_error().decode())
+    return f, fields
 
 
 class Batch:

@@ -190,6 +190,7 @@ struct oshun_ctx {
 
     CoefLM* d_coef = nullptr;
     int* d_plane_of = nullptr;   // [(l0+1)*(m0+1)]
+    std::vector<int> plane_of_host;   // the same map on the host
     int* d_plane_l = nullptr;    // [nplanes]
     int* d_plane_m = nullptr;    // [nplanes]
     int* d_hplane = nullptr;     // [2*nh]: plane of Re (or -1 for f00), complex flag
@@ -202,6 +203,8 @@ struct oshun_ctx {
     double* d_jw = nullptr;      // [cells][3][8] current partial sums of the pipelined stage
     Clock* d_clock = nullptr;
     double2* d_stage = nullptr;  // host-layout staging for transfers and slopes
+    double* d_mom_tab = nullptr; // moments: p, 1/gamma, pow tables [7][np] (built on first use)
+    float* d_mom = nullptr;      // moments: [kMomCount + 1][cells] (the last plane is scratch)
 
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -475,6 +478,7 @@ int build_tables(oshun_ctx* h) {
     CK(cudaMalloc(&h->d_plane_of, plane_bytes));
     CK(cudaMemset(h->d_plane_of, 0xff, plane_bytes));
     CK(cudaMemcpy(h->d_plane_of, plane_of.data(), sizeof(int) * plane_of.size(), cudaMemcpyHostToDevice));
+    h->plane_of_host = plane_of;
     const size_t npl = std::max<size_t>(1, plane_l.size());
     CK(cudaMalloc(&h->d_plane_l, sizeof(int) * npl));
     CK(cudaMalloc(&h->d_plane_m, sizeof(int) * npl));
@@ -609,6 +613,7 @@ void free_ctx(oshun_ctx* h) {
     cudaFree(h->d_coef); cudaFree(h->d_plane_of); cudaFree(h->d_plane_l); cudaFree(h->d_plane_m);
     cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
     cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage); cudaFree(h->d_jw);
+    cudaFree(h->d_mom_tab); cudaFree(h->d_mom);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -874,6 +879,76 @@ int oshun_step(oshun_handle h, int nsteps, int collisions) {
             h->t_eb = h->t;
         }
     }
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_get_config(oshun_handle h, oshun_cfg* cfg) {
+    if (!h || !cfg) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    *cfg = h->cfg;
+    return OSHUN_OK;
+}
+
+int oshun_moments(oshun_handle h, float* out) {
+    if (!h || !out) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    const oshun_cfg& c = h->cfg;
+    const int np = c.nump;
+    if (!h->d_mom) {
+        // momentum tables with the host's pow(), the function the reference
+        // calls (def-Parallel.cpp:1693-1696, 1741-1750, 1815-1823, 2107-2118)
+        std::vector<double> t((size_t)7 * np);
+        for (int i = 0; i < np; ++i) {
+            const double p = axis_point(i, np, c.pmin, c.pmax);
+            const double ig = 1.0 / std::sqrt(1.0 + p * p);
+            t[i] = p;
+            t[np + i] = ig;
+            t[2 * np + i] = std::pow(ig, 2);
+            t[3 * np + i] = std::pow(ig, 3);
+            t[4 * np + i] = std::pow(p, 3);
+            t[5 * np + i] = std::pow(p, 4);
+            t[6 * np + i] = std::pow(p, 5);
+        }
+        CK(cudaMalloc(&h->d_mom_tab, sizeof(double) * t.size()));
+        CK(cudaMemcpy(h->d_mom_tab, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&h->d_mom, sizeof(float) * (kMomCount + 1) * h->cells));
+    }
+    MomentArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.f00 = h->f00[h->cur];
+    a.planes = h->pl[h->cur];
+    a.cells = h->cells; a.pstride = h->pstride;
+    a.np = np; a.nx = c.numx; a.ny = c.numy;
+    auto plane = [&](int l, int m) {
+        return (l <= c.l0 && m <= c.m0) ? (int)(h->plane_of_host[(size_t)l * (c.m0 + 1) + m]) : -2;
+    };
+    a.q10 = plane(1, 0); a.q11 = plane(1, 1); a.q20 = plane(2, 0); a.q21 = plane(2, 1); a.q22 = plane(2, 2);
+    const double* T = h->d_mom_tab;
+    a.pr = T; a.invgamma = T + np; a.ig2 = T + 2 * np; a.ig3 = T + 3 * np;
+    a.pow3 = T + 4 * np; a.pow4 = T + 5 * np; a.pow5 = T + 6 * np;
+    const double p0 = axis_point(0, np, c.pmin, c.pmax), p1 = axis_point(1, np, c.pmin, c.pmax);
+    const double dp = p1 - p0;
+    a.dp = dp;
+    a.p0p1_sq = p0 * p0 / (p1 * p1);
+    a.inv_mp0p1_sq = 1.0 / (1.0 - a.p0p1_sq);
+    a.corr5 = std::pow(p0, 5) / (dp * p1 * 5.0);
+    a.corr7 = std::pow(p0, 7) / (dp * p1 * 7.0);
+    a.density_np = c.density_np; a.Zeta = c.Zeta;
+    a.nu_pre = std::sqrt(2.0 / M_PI) / 9.0;
+    a.s_dens = (float)(4.0 * M_PI * dp);
+    a.s_v1 = (float)((4.0 * M_PI / 3.0) * dp);
+    a.s_v2 = (float)((8.0 * M_PI / 3.0) * dp);
+    a.s_m2 = (float)(8.0 * M_PI / 15.0 * dp);
+    a.s_vyvy = (float)(16.0 * M_PI / 5.0 * dp);
+    a.s_vxvy = (float)(8.0 * M_PI / 5.0 * dp);
+    a.s_vxvz = (float)(-(8.0 * M_PI / 5.0) * dp);
+    a.s_vyvz = (float)(-(16.0 * M_PI / 5.0) * dp);
+    a.s_pre = (float)(2.73785179e-19 * c.density_np);
+    a.s_kx = (float)(0.5 / (axis_point(0, c.numx, c.xmin, c.xmax) - axis_point(1, c.numx, c.xmin, c.xmax)));
+    a.s_ky = c.numy > 1 ? (float)(0.5 / (axis_point(0, c.numy, c.ymin, c.ymax) - axis_point(1, c.numy, c.ymin, c.ymax)))
+                        : 0.0f;
+    a.out = h->d_mom;
+    CK(launch_moments(a, h->fp32 ? 1 : 0, h->stream));
+    CK(cudaMemcpyAsync(out, h->d_mom, sizeof(float) * kMomCount * h->cells, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return OSHUN_OK;
 }

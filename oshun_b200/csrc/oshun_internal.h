@@ -164,6 +164,26 @@ cudaError_t launch_nan_check(const double* f00, const void* planes, int planes_f
                              long long n_planes, const void* fields, long long n_fields, int* status,
                              cudaStream_t s);
 
+// Moments of Parallel_Output::nonrelativistic_moments (moments.cu); output
+// planes [kMomCount][numy][numx] in this order (the public oshun_moment enum)
+enum { kMomN = 0, kMomVx, kMomVy, kMomVxVx, kMomVyVy, kMomVzVz, kMomVxVy, kMomVxVz, kMomVyVz, kMomVsq, kMomT, kMomP,
+       kMomND, kMomNu, kMomQx, kMomKx, kMomQy, kMomKy, kMomCount };
+struct MomentArgs {
+    const double* f00;    // FP64 f00 plane
+    const void* planes;   // l >= 1 planes (double or float)
+    long long cells, pstride;
+    int np, nx, ny;
+    int q10, q11, q20, q21, q22;   // plane of Re f_lm, -2 when the harmonic is absent
+    // momentum tables [np]: p, 1/gamma, and the host's pow() of the reference's moments
+    const double *pr, *invgamma, *ig2, *ig3, *pow3, *pow4, *pow5;
+    double dp, p0p1_sq, inv_mp0p1_sq, corr5, corr7;
+    double density_np, Zeta, nu_pre;
+    // scalings rounded to float as Matrix2D<float> *= <double> does
+    float s_dens, s_v1, s_v2, s_m2, s_vyvy, s_vxvy, s_vxvz, s_vyvz, s_pre, s_kx, s_ky;
+    float* out;           // [kMomCount + 1][cells]: the moments, then a scratch plane
+};
+cudaError_t launch_moments(const MomentArgs& a, int planes_fp32, cudaStream_t s);
+
 void set_error(const std::string& msg);
 
 // Raises a kernel's dynamic shared-memory limit to `bytes` on the current
