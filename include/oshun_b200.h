@@ -126,13 +126,36 @@ int oshun_collide_flm(oshun_handle h, double t_new);
  * CUDA graph once captured.  `collisions` = 0 skips the collision calls. */
 int oshun_step(oshun_handle h, int nsteps, int collisions);
 
+/* nsteps of the reference's small step with the implicit electric field
+ * (OSHUN-1/main.cpp:77-107 with implicit_E; Runge_Kutta_2_Imp, def-RK.cpp:
+ * 399-588; Implicit_E_Field, def-ImplicitE.cpp:471-676), cfg.dt the RK2 step h.
+ * mask selects the calls of each step, in this order (63 = the whole step):
+ *    1  rk.advance_p1   RK2 of advection, B and Faraday (Implicit_Actions::Adv1)
+ *    2  ee.loop(t)      f00 e-e collisions
+ *   16  em.advance      the implicit E: probes of the collisional plasma's
+ *                       response to DE = sqrt(eps)|E| + eps in each component
+ *                       (their RK2 effect on l <= 2 and the f1 solve), the
+ *                       finite-difference conductivity tensor and a 3x3 solve
+ *                       per cell for the E whose current matches rot B (1D,
+ *                       if_implicit1D: Ex with zero current), up to 4 attempts
+ *   32  rk.advance_p2   RK2 of the new E's couplings (Adv2) and CLEAN_LOW_PC
+ *    4  eb.advance_1(t) implicit f1 collisions
+ *    8  eb.advance_lm(t) implicit f_lm collisions
+ * The probe's finite differences amplify rounding by about 1/sqrt(16 eps):
+ * results agree with the reference to the reference's own sensitivity to a
+ * 1-ulp change of its input (about 1e-8 relative).  Returns OSHUN_ERR_NUMERIC
+ * where the reference exits (a zero determinant left in more than 8 cells). */
+int oshun_rk2_imp_step(oshun_handle h, int nsteps, int mask);
+
 /* ---- queries -------------------------------------------------------------- */
 
 /* RK clock (Runge_Kutta_4::time, OSHUN-1/def-RK.cpp:76). */
 int oshun_time(oshun_handle h, double* t);
 /* Status word: bit 0 = a Gauss-Seidel solve found its matrix not diagonally
  * dominant and kept f (the reference's WARNING, def-FokkerPlanck.cpp:1027-1030);
- * bit 1 = NaN/Inf in the state (checked by this call); bit 4 = a pipeline wait
+ * bit 1 = NaN/Inf in the state (checked by this call); bit 2 = an implicit-E
+ * solve left cells with a zero determinant after its 4 attempts (the
+ * reference's WARNING, def-ImplicitE.cpp:666-669); bit 4 = a pipeline wait
  * of a stage launch gave up (that launch returned without finishing: the state
  * is undefined).  *count = skipped solves since the last call.  Reading clears
  * the word. */

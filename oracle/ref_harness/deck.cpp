@@ -35,7 +35,7 @@ Inputdata::input_list::input_list() {
     ymin = g_deck.ymin; ymax = g_deck.ymax;
     pmin = g_deck.pmin; pmax = g_deck.pmax;
     clf_dp = g_deck.clf_dp;
-    if_implicitES = false;
+    if_implicitES = false;   // the implicit-E path solves the full electromagnetic case
     if_implicit1D = g_deck.if_implicit1D != 0;
     small_dt = g_deck.small_dt;
     smaller_dt = g_deck.small_dt;

@@ -15,6 +15,11 @@
 //   step:N[:MASK]    N time steps of the main loop order (main.cpp:77-107):
 //                    MASK bit 1 rk4.advance_p1, 2 ee.loop, 4 eb.advance_1,
 //                    8 eb.advance_lm; default 15
+//   istep:N[:MASK]   N time steps of the implicit-E main loop (main.cpp:77-107
+//                    with implicit_E): MASK bit 1 Runge_Kutta_2_Imp::advance_p1,
+//                    2 ee.loop, 16 Implicit_E_Field::advance (def-ImplicitE.cpp:
+//                    471-676), 32 advance_p2, 4 eb.advance_1, 8 eb.advance_lm;
+//                    default 63
 //   time             print the wall time of the step loops to stdout
 //   restart_write:R:S  Restart_Facility::Write(R, S, Y) (def-Export.cpp:768-800):
 //                    RESTART/re_<R>_<S>.dat in the working directory
@@ -59,6 +64,7 @@
 #include <fstream>
 #include <sstream>
 #include <mpi.h>
+#include "decl-implicitE.h"
 #include "decl-output.h"
 #include "decl-export.h"
 #include "decl-parallel.h"
@@ -271,6 +277,28 @@ int main(int argc, char** argv) {
                 if (mask & 2) ee.loop(tnew);
                 if (mask & 4) eb.advance_1(tnew);
                 if (mask & 8) eb.advance_lm(tnew);
+                refresh_guards(Y);
+            }
+            elapsed += now_s() - t0;
+        } else if (op.compare(0, 6, "istep:") == 0) {
+            int nsteps = 0, mask = 63;
+            if (std::sscanf(op.c_str() + 6, "%d:%d", &nsteps, &mask) < 1) {
+                std::fprintf(stderr, "oshun_ref: bad op %s\n", op.c_str());
+                return 2;
+            }
+            Runge_Kutta_2_Imp rk(Y, 0);
+            Explicit_EC_FP ee(Y, 0);
+            Euler_Backward eb(Y, 0);
+            Electric_Field_Methods::Implicit_E_Field em(Y, 0);
+            double t0 = now_s();
+            for (int s = 0; s < nsteps; ++s) {
+                if (mask & 1) rk.advance_p1();
+                refresh_guards(Y);   // the single-node image of Neighbor_ImplicitE_Communications
+                if (mask & 2) ee.loop(rk.time());
+                if (mask & 16) em.advance(&rk, &eb);
+                if (mask & 32) rk.advance_p2();
+                if (mask & 4) eb.advance_1(rk.time());
+                if (mask & 8) eb.advance_lm(rk.time());
                 refresh_guards(Y);
             }
             elapsed += now_s() - t0;

@@ -33,7 +33,7 @@ EXPORTED = [
     "oshun_adjoint_create", "oshun_adjoint_destroy", "oshun_adjoint_set_stream", "oshun_adjoint_state_size",
     "oshun_adjoint_forward", "oshun_adjoint_vjp", "oshun_debug_inject_stage_timeout", "oshun_get_config",
     "oshun_moments", "oshun_restart_bytes", "oshun_restart_pack", "oshun_restart_unpack", "oshun_restart_write",
-    "oshun_restart_read",
+    "oshun_restart_read", "oshun_rk2_imp_step",
 ]
 
 
@@ -89,6 +89,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_plane_index.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.oshun_debug_inject_stage_timeout.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     lib.oshun_get_config.argtypes = [vp, ctypes.POINTER(OshunCfg)]
+    lib.oshun_rk2_imp_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.oshun_moments.argtypes = [vp, vp]
     lib.oshun_restart_bytes.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int]
     lib.oshun_restart_bytes.restype = ctypes.c_longlong
@@ -220,6 +221,10 @@ class Handle:
 
     def step(self, nsteps: int, collisions: bool = True) -> None:
         self._check(self.lib.oshun_step(self._h, nsteps, 1 if collisions else 0), "oshun_step")
+
+    def rk2_imp_step(self, nsteps: int, mask: int = 63) -> None:
+        """nsteps of the implicit-E small step (mask bits as oshun_rk2_imp_step)."""
+        self._check(self.lib.oshun_rk2_imp_step(self._h, nsteps, mask), "oshun_rk2_imp_step")
 
     def synchronize(self) -> None:
         self._check(self.lib.oshun_synchronize(self._h), "oshun_synchronize")

@@ -18,6 +18,7 @@
 // is the accumulator Y that becomes the new state, sets 2 and 3 carry the
 // stage inputs.  `cur` and `nxt` swap after each step.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -203,6 +204,16 @@ struct oshun_ctx {
     double* d_jw = nullptr;      // [cells][3][8] current partial sums of the pipelined stage
     Clock* d_clock = nullptr;
     double2* d_stage = nullptr;  // host-layout staging for transfers and slopes
+    std::vector<CoefLM> coef_host;   // the coupling table on the host
+    // implicit electric field (built on first use): coupling tables of
+    // ImpEx, ImpEx1D, ImpEy/z and Exyz1D; J0, J(DEx), J(DEy), J(DEz), JN, DE,
+    // EN ([3][cells] each) and p^3/gamma; the probe field; the zero count
+    CoefLM* d_coef_imp[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* d_imp = nullptr;
+    void* d_fe = nullptr;
+    int* d_zeros = nullptr;
+    int imp_zeros = 0;           // cells left with a zero determinant by the last implicit-E solve
+    bool imp_zero_seen = false;  // some implicit-E solve since the last status read left one
     double* d_mom_tab = nullptr; // moments: p, 1/gamma, pow tables [7][np] (built on first use)
     float* d_mom = nullptr;      // moments: [kMomCount + 1][cells] (the last plane is scratch)
 
@@ -322,6 +333,7 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     a.g00_s = g00_s; a.g00_inv = g00_inv; a.g00_gr = g00_gr;
     a.idx = idx; a.idy = idy;
     a.seq = d_seq; a.nh = nh; a.err = d_status;
+    a.parts = kPartAll;
     a.wait_ns = inject_active ? inject_wait_ns : 1000000000ull;
     a.withhold = inject_active ? inject_withhold : -1;
     a.jw = d_jw;
@@ -473,6 +485,7 @@ int build_tables(oshun_ctx* h) {
 
     CK(cudaMalloc(&h->d_coef, sizeof(CoefLM) * coef.size()));
     CK(cudaMemcpy(h->d_coef, coef.data(), sizeof(CoefLM) * coef.size(), cudaMemcpyHostToDevice));
+    h->coef_host = coef;
     // padded to 16 bytes: batched launches bulk-copy the map
     const size_t plane_bytes = (sizeof(int) * plane_of.size() + 15) / 16 * 16;
     CK(cudaMalloc(&h->d_plane_of, plane_bytes));
@@ -534,13 +547,15 @@ int enqueue_rk4(oshun_ctx* h) {
     return OSHUN_OK;
 }
 
-CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt) {
+CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub, double hsub, double Dt,
+                         int set = -1) {
     CollideArgs a;
     std::memset(&a, 0, sizeof(a));
     const oshun_cfg& c = h->cfg;
     const int np = c.nump;
-    a.f00 = h->f00[h->cur];
-    a.planes = h->pl[h->cur];
+    if (set < 0) set = h->cur;
+    a.f00 = h->f00[set];
+    a.planes = h->pl[set];
     a.planes_fp32 = h->fp32 ? 1 : 0;
     a.plane_of = h->d_plane_of; a.plane_l = h->d_plane_l; a.plane_m = h->d_plane_m;
     a.nplanes = h->nplanes;
@@ -605,6 +620,185 @@ void collide_params(const oshun_ctx* h, double t_new, int* nsub, double* hsub, d
     *Dt = t_new - h->t_eb;                                     // def-FokkerPlanck.cpp:1277,1297
 }
 
+// ---- implicit electric field: Runge_Kutta_2_Imp and Implicit_E_Field ----
+
+// The coupling tables of the implicit actions, subsets of the explicit E
+// couplings (same closed-form coefficients):
+//   [0] ImpEx    Ex G from (0,0) (1,0) (1,1), Ex H from (1,0) (2,0) (3,0) (2,1) (3,1)
+//                (ElectricField::Implicit_Ex, def-VlasovMax.cpp:157-198)
+//   [1] ImpEx1D  the m = 0 part of [0] (Implicit_Ex1D, :202-228)
+//   [2] ImpEy/z  every E_+- coupling into l <= 2 (Implicit_Eyz, :233-292)
+//   [3] Exyz1D   Ex couplings among m = 0 harmonics (Exyz1D, :299-341)
+int build_implicit(oshun_ctx* h) {
+    const oshun_cfg& c = h->cfg;
+    const int l0 = c.l0, m0 = c.m0, np = c.nump;
+    auto keep = [&](int l, int m, int which) {
+        CoefLM k{};
+        const CoefLM& e = h->coef_host[(size_t)l * (m0 + 1) + m];
+        k.gfac = e.gfac; k.invpax = e.invpax; k.hp0 = e.hp0;
+        auto in = [&](std::initializer_list<std::pair<int, int>> lst) {
+            for (auto& q : lst)
+                if (q.first == l && q.second == m) return true;
+            return false;
+        };
+        switch (which) {
+            case 0:
+                if (in({{0, 0}, {1, 0}, {1, 1}})) k.ex_g = e.ex_g;
+                if (in({{1, 0}, {2, 0}, {3, 0}, {2, 1}, {3, 1}})) k.ex_h = e.ex_h;
+                break;
+            case 1:
+                if (in({{0, 0}, {1, 0}})) k.ex_g = e.ex_g;
+                if (in({{1, 0}, {2, 0}, {3, 0}})) k.ex_h = e.ex_h;
+                break;
+            case 2:
+                if (in({{0, 0}, {1, 0}, {1, 1}})) k.em_g = e.em_g;
+                if (in({{2, 0}, {3, 0}, {3, 1}})) k.em_h = e.em_h;
+                if (in({{1, 1}, {2, 1}, {3, 1}, {2, 2}, {3, 2}}) || (m0 > 2 && l == 3 && m == 3)) k.ep_h = e.ep_h;
+                if (in({{1, 1}})) k.ep_g = e.ep_g;
+                break;
+            default:
+                if (m == 0) { k.ex_g = e.ex_g; k.ex_h = e.ex_h; }
+                break;
+        }
+        return k;
+    };
+    for (int which = 0; which < 4; ++which) {
+        std::vector<CoefLM> t((size_t)(l0 + 1) * (m0 + 1));
+        std::memset(t.data(), 0, sizeof(CoefLM) * t.size());
+        for (int l = 0; l <= l0; ++l)
+            for (int m = 0; m <= std::min(l, m0); ++m) t[(size_t)l * (m0 + 1) + m] = keep(l, m, which);
+        CK(cudaMalloc(&h->d_coef_imp[which], sizeof(CoefLM) * t.size()));
+        CK(cudaMemcpy(h->d_coef_imp[which], t.data(), sizeof(CoefLM) * t.size(), cudaMemcpyHostToDevice));
+    }
+    // p^3/gamma of Current_xyz (def-ImplicitE.cpp:59-69)
+    std::vector<double> w(np);
+    for (int i = 0; i < np; ++i) {
+        const double p = axis_point(i, np, c.pmin, c.pmax);
+        w[i] = (p * p) * (p / std::sqrt(1.0 + p * p));
+    }
+    CK(cudaMalloc(&h->d_imp, sizeof(double) * ((size_t)21 * h->cells + np)));
+    CK(cudaMemcpy(h->d_imp + 21 * h->cells, w.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_fe, h->ts * 6 * (size_t)h->cells));
+    CK(cudaMalloc(&h->d_zeros, sizeof(int)));
+    return OSHUN_OK;
+}
+
+ImplicitArgs implicit_args(const oshun_ctx* h) {
+    const oshun_cfg& c = h->cfg;
+    ImplicitArgs a;
+    std::memset(&a, 0, sizeof(a));
+    for (int i = 0; i < 4; ++i) a.planes[i] = h->pl[i];
+    a.cells = h->cells; a.pstride = h->pstride;
+    a.np = c.nump; a.nx = c.numx; a.ny = c.numy;
+    a.q10 = h->plane_of_host[(size_t)(c.m0 + 1)];
+    a.q11 = c.m0 >= 1 ? h->plane_of_host[(size_t)(c.m0 + 1) + 1] : -1;
+    a.fp32 = h->fp32 ? 1 : 0;
+    a.one_d = c.if_implicit1D ? 1 : 0;
+    a.p3og = h->d_imp + 21 * h->cells;
+    const double p0 = axis_point(0, c.nump, c.pmin, c.pmax), p1 = axis_point(1, c.nump, c.pmin, c.pmax);
+    double small = p0;
+    small *= small; small *= small; small *= p0; small *= 0.2; small *= 1.0 / p1;
+    a.dp = h->dp; a.small = small;
+    a.c4 = (-4.0) * M_PI / 3.0;
+    a.c8 = (-8.0) * M_PI / 3.0;
+    a.idx = h->idx; a.idy = h->idy;
+    a.eps = 16.0 * DBL_EPSILON;
+    a.large_eps = std::sqrt(a.eps);
+    return a;
+}
+
+// one stage launch of a partial right-hand side (the implicit actions)
+int launch_stage_part(oshun_ctx* h, int in_set, int B_set, int A_set, int out_set, int first, double c1, double c2,
+                      int parts, const CoefLM* coef, const void* fld_in) {
+    cudaError_t e;
+    if (h->fp32) {
+        StageArgs<float> a = h->stage_args<float>(in_set, out_set, 0);
+        a.f00_B = h->f00[B_set]; a.pl_B = (const float*)h->pl[B_set]; a.fld_B = (const float*)h->fld[B_set];
+        a.f00_A = h->f00[A_set]; a.pl_A = (float*)h->pl[A_set]; a.fld_A = (float*)h->fld[A_set];
+        if (out_set >= 0) { a.f00_out = h->f00[out_set]; a.pl_out = (float*)h->pl[out_set]; a.fld_out = (float*)h->fld[out_set]; }
+        a.first = first; a.c1 = c1; a.c2 = c2; a.parts = parts; a.coef = coef;
+        if (fld_in) a.fld_in = (const float*)fld_in;
+        e = launch_stage_fp32(a, h->mc, h->stream);
+    } else {
+        StageArgs<double> a = h->stage_args<double>(in_set, out_set, 0);
+        a.f00_B = h->f00[B_set]; a.pl_B = (const double*)h->pl[B_set]; a.fld_B = (const double*)h->fld[B_set];
+        a.f00_A = h->f00[A_set]; a.pl_A = (double*)h->pl[A_set]; a.fld_A = (double*)h->fld[A_set];
+        if (out_set >= 0) { a.f00_out = h->f00[out_set]; a.pl_out = (double*)h->pl[out_set]; a.fld_out = (double*)h->fld[out_set]; }
+        a.first = first; a.c1 = c1; a.c2 = c2; a.parts = parts; a.coef = coef;
+        if (fld_in) a.fld_in = (const double*)fld_in;
+        e = launch_stage_fp64(a, h->mc, h->stream);
+    }
+    if (e != cudaSuccess) { set_error(std::string("rk2 stage launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+    return OSHUN_OK;
+}
+
+// One Runge_Kutta_2_Imp update (def-RK.cpp:463-493 and the advance_IE*
+// forms, :515-588) from set S into set T through set U:
+//   Y0 = Y; Yh = F(Y0) h; Y0 += Yh; Yh *= 0.5; Y += Yh; Yh = F(Y0) h/2; Y += Yh
+int enqueue_rk2(oshun_ctx* h, int S, int T, int U, int parts, const CoefLM* coef, const void* fld_in) {
+    const double dt = h->cfg.dt;
+    int rc = launch_stage_part(h, S, S, T, U, 1, dt, 0.5, parts, coef, fld_in);
+    if (rc) return rc;
+    return launch_stage_part(h, U, S, T, -1, 0, 0.5 * dt, 1.0, parts, coef, fld_in);
+}
+
+// Implicit_E_Field::advance (def-ImplicitE.cpp:471-676) on set cur at RK time t
+int enqueue_implicit_e(oshun_ctx* h) {
+    int rc;
+    if (!h->d_imp && (rc = build_implicit(h))) return rc;
+    const ImplicitArgs ia = implicit_args(h);
+    const long long C = h->cells;
+    double* J0 = h->d_imp;
+    double* JX = J0 + 3 * C;
+    double* JY = J0 + 6 * C;
+    double* JZ = J0 + 9 * C;
+    double* JN = J0 + 12 * C;
+    double* DE = J0 + 15 * C;
+    double* EN = J0 + 18 * C;
+    const int S = h->cur, W = h->cur ^ 1, U = 3;
+    const bool one_d = ia.one_d != 0;
+    int nsub; double hsub, Dt;
+    collide_params(h, h->t, &nsub, &hsub, &Dt);
+    // Euler_Backward::advance_1 of a probe state, then its current
+    auto collide_and_current = [&](double* J) -> int {
+        int r = launch_collide_args(h, collide_args(h, 0, 1, 0, nsub, hsub, Dt, W));
+        if (r) return r;
+        CK(launch_implicit_current(ia, W, J, h->stream));
+        return OSHUN_OK;
+    };
+    CK(launch_implicit_find_de(ia, h->fld[S], DE, h->stream));
+    int zeros = 0;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        CK(cudaMemsetAsync(h->d_zeros, 0, sizeof(int), h->stream));
+        // E = 0: the probe state is the state itself (its f00 and l = 1 planes)
+        CK(cudaMemcpyAsync(h->f00[W], h->f00[S], sizeof(double) * h->pstride, cudaMemcpyDeviceToDevice, h->stream));
+        const int q1 = ia.q10, n1 = ia.q11 >= 0 ? 3 : 1;
+        CK(cudaMemcpyAsync((char*)h->pl[W] + h->ts * (size_t)q1 * h->pstride,
+                           (const char*)h->pl[S] + h->ts * (size_t)q1 * h->pstride,
+                           h->ts * (size_t)n1 * h->pstride, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = collide_and_current(J0))) return rc;
+        // the probes: E = DE in one component, its RK2 effect on l <= 2, collisions, current
+        const int ncomp = one_d ? 1 : 3;
+        double* Jp[3] = {JX, JY, JZ};
+        for (int comp = 0; comp < ncomp; ++comp) {
+            CK(launch_implicit_probe_field(ia, DE, comp, h->d_fe, h->stream));
+            const CoefLM* tab = comp == 0 ? h->d_coef_imp[one_d ? 1 : 0] : h->d_coef_imp[2];
+            const int part = comp == 0 ? kPartEx : (comp == 1 ? kPartEy : kPartEz);
+            if ((rc = enqueue_rk2(h, S, W, U, part, tab, h->d_fe))) return rc;
+            if ((rc = collide_and_current(Jp[comp]))) return rc;
+        }
+        if (!one_d) CK(launch_implicit_ampere(ia, h->fld[S], JN, h->stream));
+        CK(launch_implicit_solve(ia, J0, JX, JY, JZ, JN, DE, EN, h->d_zeros, h->stream));
+        CK(cudaMemcpyAsync(&zeros, h->d_zeros, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (zeros == 0) break;
+    }
+    CK(launch_implicit_set_e(ia, EN, h->fld[S], h->stream));
+    h->imp_zeros = zeros;
+    if (zeros > 0) h->imp_zero_seen = true;   // status bit 2 until the word is read
+    return OSHUN_OK;
+}
+
 void free_ctx(oshun_ctx* h) {
     for (int p = 0; p < 2; ++p)
         for (int c = 0; c < 2; ++c)
@@ -614,6 +808,8 @@ void free_ctx(oshun_ctx* h) {
     cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
     cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage); cudaFree(h->d_jw);
     cudaFree(h->d_mom_tab); cudaFree(h->d_mom);
+    for (int i = 0; i < 4; ++i) cudaFree(h->d_coef_imp[i]);
+    cudaFree(h->d_imp); cudaFree(h->d_fe); cudaFree(h->d_zeros);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -883,6 +1079,60 @@ int oshun_step(oshun_handle h, int nsteps, int collisions) {
     return OSHUN_OK;
 }
 
+int oshun_rk2_imp_step(oshun_handle h, int nsteps, int mask) {
+    if (!h || nsteps < 0) return OSHUN_ERR_ARG;
+    if (mask < 0 || mask > 63) { set_error("mask: bits 1, 2, 4, 8, 16, 32"); return OSHUN_ERR_ARG; }
+    if (!h->d_imp) {
+        const int rc = build_implicit(h);
+        if (rc) return rc;
+    }
+    int rc;
+    for (int s = 0; s < nsteps; ++s) {
+        if (mask & 1) {
+            // Runge_Kutta_2_Imp::advance_p1: Adv1 = advection + B + Faraday (def-Actions.cpp:117-133)
+            if ((rc = enqueue_rk2(h, h->cur, h->cur ^ 1, 3, kPartB | kPartAdv | kPartFaraday, h->d_coef, nullptr)))
+                return rc;
+            h->cur ^= 1;
+            h->t += h->cfg.dt;
+        }
+        if (mask & 2) {
+            int nsub; double hsub, Dt;
+            collide_params(h, h->t, &nsub, &hsub, &Dt);
+            if ((rc = enqueue_collide(h, 1, 0, 0, nsub, hsub, Dt))) return rc;
+            h->t_ee = h->t;
+        }
+        if (mask & 16) {
+            if ((rc = enqueue_implicit_e(h))) return rc;
+            if (h->imp_zeros > 8) {
+                set_error("implicit E: zero determinant in " + std::to_string(h->imp_zeros) +
+                          " cells after 4 attempts (the reference stops here)");
+                return OSHUN_ERR_NUMERIC;
+            }
+        }
+        if (mask & 32) {
+            // advance_p2: Adv2 = the new E's couplings + CLEAN_LOW_PC (def-Actions.cpp:137-160)
+            const bool one_d = h->cfg.if_implicit1D != 0;
+            const int parts = (one_d ? kPartEx : (kPartEx | kPartEy | kPartEz)) | kPartClean;
+            if ((rc = enqueue_rk2(h, h->cur, h->cur ^ 1, 3, parts, one_d ? h->d_coef_imp[3] : h->d_coef, nullptr)))
+                return rc;
+            h->cur ^= 1;
+        }
+        if (mask & 12) {
+            int nsub; double hsub, Dt;
+            collide_params(h, h->t, &nsub, &hsub, &Dt);
+            if ((mask & 4) && (rc = enqueue_collide(h, 0, 1, 0, nsub, hsub, Dt))) return rc;
+            if (mask & 8) {
+                if ((rc = enqueue_collide(h, 0, 0, 1, nsub, hsub, Dt))) return rc;
+                h->t_eb = h->t;
+            }
+        }
+    }
+    Clock ck{h->t, h->t_ee, h->t_eb};
+    CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
 int oshun_get_config(oshun_handle h, oshun_cfg* cfg) {
     if (!h || !cfg) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
     *cfg = h->cfg;
@@ -979,8 +1229,9 @@ int oshun_status_flags(oshun_handle h, int* flags, long long* count) {
     CK(cudaMemcpyAsync(st, h->d_status, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * 2, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (flags) *flags = st[0];
+    if (flags) *flags = st[0] | (h->imp_zero_seen ? 4 : 0);
     if (count) *count = st[1];
+    h->imp_zero_seen = false;
     return OSHUN_OK;
 }
 

@@ -36,6 +36,21 @@ struct alignas(16) CoefLM {
 };
 static_assert(sizeof(CoefLM) == 128 && alignof(CoefLM) == 16, "CoefLM layout");
 
+// Parts of the right-hand side a stage launch evaluates.  Actions::Adv
+// (def-Actions.cpp:73-94) is every part; the implicit-E actions
+// (Implicit_Actions, def-Actions.cpp:117-218) are subsets: Adv1 = B +
+// advection + Faraday, Adv2 = E + CLEAN_LOW_PC, ImpEx/y/z = one E component
+// with a restricted coupling table.
+enum : int {
+    kPartEx = 1, kPartEy = 2, kPartEz = 4,   // E couplings, per component of the stage-input field
+    kPartB = 8,                              // B couplings
+    kPartAdv = 16,                           // x and y advection
+    kPartAmpere = 32,                        // dE/dt: current and rot B
+    kPartFaraday = 64,                       // dB/dt: -rot E
+    kPartClean = 128,                        // CLEAN_LOW_PC on the slope
+    kPartAll = 255
+};
+
 // Arguments of one fused RHS + RK4 stage launch.  TS is the storage and
 // arithmetic type of the l >= 1 planes and the fields; f00 is always FP64.
 template <typename TS>
@@ -62,6 +77,8 @@ struct StageArgs {
     int nh;
     int* err;             // error word (bit 4: a pipeline wait timed out)
     unsigned long long wait_ns;   // a pipeline wait gives up after this many ns (single-problem kernel)
+    int parts;            // kPart* bits of the RHS evaluated (kPartAll: Actions::Adv); any other
+                          // set runs the global-load kernel (the implicit-E actions)
     int withhold;         // fault injection for tests: CTA 0's source producer skips this copy (-1: none)
     const void* coef_ts;  // coupling table in the arithmetic type (batched launches)
     double* jw;           // [cells][3][8]: per-warp partial sums of Jx, Re Jy, Im Jy (single-problem pipeline)
@@ -183,6 +200,30 @@ struct MomentArgs {
     float* out;           // [kMomCount + 1][cells]: the moments, then a scratch plane
 };
 cudaError_t launch_moments(const MomentArgs& a, int planes_fp32, cudaStream_t s);
+
+// Implicit electric field (implicit_e.cu): per-cell kernels of
+// Implicit_E_Field::advance; the probe states come from the stage and
+// collision kernels
+struct ImplicitArgs {
+    const void* planes[4];   // l >= 1 planes of each state set (double or float)
+    long long cells, pstride;
+    int np, nx, ny;
+    int q10, q11;            // planes of f10 and Re f11 (-1: absent)
+    int fp32;
+    int one_d;               // if_implicit1D: Ex alone, no Ampere
+    const double* p3og;      // p^3/gamma [np]
+    double dp, small, c4, c8;   // quadrature step, p0 correction, -4 pi/3, -8 pi/3
+    double idx, idy;         // -1/(2 dx), -1/(2 dy)
+    double eps, large_eps;   // 16 DBL_EPSILON and its square root
+};
+cudaError_t launch_implicit_current(const ImplicitArgs& a, int set, double* J, cudaStream_t s);
+cudaError_t launch_implicit_ampere(const ImplicitArgs& a, const void* fields, double* JN, cudaStream_t s);
+cudaError_t launch_implicit_find_de(const ImplicitArgs& a, const void* fields, double* DE, cudaStream_t s);
+cudaError_t launch_implicit_probe_field(const ImplicitArgs& a, const double* DE, int comp, void* FE, cudaStream_t s);
+cudaError_t launch_implicit_solve(const ImplicitArgs& a, const double* J0, const double* JX, const double* JY,
+                                  const double* JZ, const double* JN, double* DE, double* EN, int* zeros,
+                                  cudaStream_t s);
+cudaError_t launch_implicit_set_e(const ImplicitArgs& a, const double* EN, void* fields, cudaStream_t s);
 
 void set_error(const std::string& msg);
 

@@ -52,18 +52,23 @@ __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long c
     const TS* F = a.fld_in;
     const long long C = a.cells;
     const TS idx = (TS)a.idx, idy = (TS)a.idy;
-    // J: Ex += Jx, Ey += Re J11, Ez += -Im J11 with J11 = 2 * (f11 quadrature)
-    TS dEx = (TS)Jx;
-    TS dEy = (TS)(2.0 * Jyr);
-    TS dEz = (TS)(-(2.0 * Jyi));
-    dEx += idy * (ld(F + 5 * C + cym) - ld(F + 5 * C + cyp));
-    dEy += -idx * (ld(F + 5 * C + cxm) - ld(F + 5 * C + cxp));
-    dEz += -idy * (ld(F + 3 * C + cym) - ld(F + 3 * C + cyp));
-    dEz += idx * (ld(F + 4 * C + cxm) - ld(F + 4 * C + cxp));
-    TS dBx = -idy * (ld(F + 2 * C + cym) - ld(F + 2 * C + cyp));
-    TS dBy = idx * (ld(F + 2 * C + cxm) - ld(F + 2 * C + cxp));
-    TS dBz = idy * (ld(F + 0 * C + cym) - ld(F + 0 * C + cyp));
-    dBz += -idx * (ld(F + 1 * C + cxm) - ld(F + 1 * C + cxp));
+    TS dEx = 0, dEy = 0, dEz = 0, dBx = 0, dBy = 0, dBz = 0;
+    if (a.parts & kPartAmpere) {
+        // J: Ex += Jx, Ey += Re J11, Ez += -Im J11 with J11 = 2 * (f11 quadrature)
+        dEx = (TS)Jx;
+        dEy = (TS)(2.0 * Jyr);
+        dEz = (TS)(-(2.0 * Jyi));
+        dEx += idy * (ld(F + 5 * C + cym) - ld(F + 5 * C + cyp));
+        dEy += -idx * (ld(F + 5 * C + cxm) - ld(F + 5 * C + cxp));
+        dEz += -idy * (ld(F + 3 * C + cym) - ld(F + 3 * C + cyp));
+        dEz += idx * (ld(F + 4 * C + cxm) - ld(F + 4 * C + cxp));
+    }
+    if (a.parts & kPartFaraday) {
+        dBx = -idy * (ld(F + 2 * C + cym) - ld(F + 2 * C + cyp));
+        dBy = idx * (ld(F + 2 * C + cxm) - ld(F + 2 * C + cxp));
+        dBz = idy * (ld(F + 0 * C + cym) - ld(F + 0 * C + cyp));
+        dBz += -idx * (ld(F + 1 * C + cxm) - ld(F + 1 * C + cxp));
+    }
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 0 * C + cell, dEx);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 1 * C + cell, dEy);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 2 * C + cell, dEz);
@@ -76,7 +81,7 @@ __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long c
 template <int MC, typename TS>
 __device__ __forceinline__ void row_epilogue(const StageArgs<TS>& a, const int* plane_of, int t, int p, bool pv,
                                              long long o, TS (&R)[MC + 1], TS (&I)[MC + 1]) {
-    const int nzero = t >= 2 ? min(t - 1, 80) : 0;
+    const int nzero = (t >= 2 && (a.parts & kPartClean)) ? min(t - 1, 80) : 0;
     const int mstride = a.m0 + 1;
 #pragma unroll
     for (int m = 0; m <= MC; ++m) {
@@ -118,13 +123,17 @@ __global__ void __launch_bounds__(256) rk_stage_kernel(const StageArgs<TS> a) {
 
     TS ex = 0, ey = 0, ez = 0, bx = 0, by = 0, bz = 0;
     if (cv) {
-        ex = ld(a.fld_in + cell);
-        ey = ld(a.fld_in + a.cells + cell);
-        ez = ld(a.fld_in + 2 * a.cells + cell);
-        bx = ld(a.fld_in + 3 * a.cells + cell);
-        by = ld(a.fld_in + 4 * a.cells + cell);
-        bz = ld(a.fld_in + 5 * a.cells + cell);
+        // the couplings of the parts not evaluated see a zero field
+        if (a.parts & kPartEx) ex = ld(a.fld_in + cell);
+        if (a.parts & kPartEy) ey = ld(a.fld_in + a.cells + cell);
+        if (a.parts & kPartEz) ez = ld(a.fld_in + 2 * a.cells + cell);
+        if (a.parts & kPartB) {
+            bx = ld(a.fld_in + 3 * a.cells + cell);
+            by = ld(a.fld_in + 4 * a.cells + cell);
+            bz = ld(a.fld_in + 5 * a.cells + cell);
+        }
     }
+    const bool adv = (a.parts & kPartAdv) != 0;
 
     double jx = 0.0, jyr = 0.0, jyi = 0.0;
 
@@ -135,7 +144,7 @@ __global__ void __launch_bounds__(256) rk_stage_kernel(const StageArgs<TS> a) {
         const long long oxm = cxm * np + p, oxp = cxp * np + p;
         const long long oym = cym * np + p, oyp = cyp * np + p;
         const TS invp = pv ? (TS)ld(a.inv_pr + p) : TS(0);
-        const TS vr = pv ? (TS)ld(a.vr + p) : TS(0);
+        const TS vr = (pv && adv) ? (TS)ld(a.vr + p) : TS(0);
         const double wj = pv ? ld(a.wj + p) : 0.0;
 
         TS ar[3][MC + 1], ai[3][MC + 1];
@@ -225,10 +234,13 @@ cudaError_t launch_mc(const StageArgs<TS>& a, cudaStream_t s) {
 
 template <typename TS>
 cudaError_t launch_stage(const StageArgs<TS>& a, int mc, cudaStream_t s) {
-    // the pipelined kernel where the shape fits it, else the global-load kernel
-    const cudaError_t e = launch_stage_pipe<TS>(a, mc, s);
-    if (e != cudaErrorNotSupported) return e;
-    (void)cudaGetLastError();
+    // the pipelined kernel where the shape fits it (the full right-hand side),
+    // else the global-load kernel
+    if (a.parts == kPartAll) {
+        const cudaError_t e = launch_stage_pipe<TS>(a, mc, s);
+        if (e != cudaErrorNotSupported) return e;
+        (void)cudaGetLastError();
+    }
     switch (mc) {
         case 0: return launch_mc<TS, 0>(a, s);
         case 1: return launch_mc<TS, 1>(a, s);

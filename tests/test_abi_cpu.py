@@ -13,7 +13,7 @@ HEADER = os.path.join(ROOT, "include", "oshun_b200.h")
 
 def declared_symbols():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(oshun_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*)\s+(oshun_\w+)\s*\(", src, re.M)))
 
 
 @pytest.fixture(scope="module")
