@@ -19,7 +19,8 @@ roofline   the fused RK4-stage kernel: algorithmic bytes per launch / its
 forms      (1 GPU, default workload) the other forms of the metric on the
            same box: the FP32/FP64 split Weibel run, the 512-problem FP32
            batch and the large FP64 1D Landau run, each with its value,
-           ms/step, roofline fraction and error against the FP64 GPU path
+           ms/step, roofline fraction and error against the FP64 GPU path,
+           and the time of one adjoint gradient of the sensitivity case
 cpu_baseline  the reference's own code (oracle/_ref, compiled from the OSHUN
            sources) on a bounded sample of the same workload, all host cores;
            per useful coefficient and raw (the reference's guard cells and
@@ -450,6 +451,43 @@ def form_single(workload: str, prec: int, steps: int, warmup: int, stream, err_s
     return out
 
 
+def form_adjoint(stream, nsteps: int = 500, every: int = 50, cell: int = 256) -> dict:
+    """The sensitivity configuration (1D, nx = 512, lmax = 2, np = 128): one
+    gradient of the time-integrated heat flux of one cell with respect to
+    every cell's initial temperature, forward and checkpointed backward
+    through the adjoint kernels (FP64), timed with CUDA events."""
+    import torch
+    from oshun_b200 import workloads
+    from oshun_b200.adjoint import Run, StepsWithCheckpoints, heat_flux_weight
+    cfg, tau, _ = workloads.sensitivity1d()
+    run = Run(**cfg)
+    w = heat_flux_weight(cfg, cell)
+
+    def grad_once():
+        t = torch.tensor(tau, device="cuda").requires_grad_(True)
+        y0 = workloads.sensitivity_state(cfg, t)
+        Q = StepsWithCheckpoints.apply(y0, run, nsteps, every, w)
+        Q.backward()
+        return t.grad
+
+    with torch.cuda.stream(stream):
+        grad_once()                      # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g = grad_once()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    run.close()
+    coefs = (cfg["l0"] + 1) * cfg["numx"] * cfg["nump"]
+    return {"workload": "sensitivity1d (nx=512, lmax=2, np=128)", "precision": "fp64", "steps": nsteps,
+            "checkpoint_every": every, "ms_per_gradient": ms,
+            "forward_steps_per_gradient": 2 * nsteps - nsteps // every, "vjp_steps_per_gradient": nsteps,
+            "value": coefs * nsteps / (ms * 1e-3), "unit": UNIT + " (forward steps of the gradient's trajectory)",
+            "grad_finite": bool(torch.isfinite(g).all().item())}
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -515,6 +553,7 @@ def run_ours(args, ws, rank, local):
         forms["landau1d_large"] = form_single("landau1d_large", 0, args.steps, fw, stream)
         forms["batch512"] = measure_batch(512, 1, args.steps, fw, stream, local, error_check=True)
         forms["batch512"].pop("_probs")
+        forms["adjoint_sensitivity"] = form_adjoint(stream)
         forms["batch512"]["speedup_vs_fp64"] = forms["batch512"]["value"] / value
 
     cpu = None
