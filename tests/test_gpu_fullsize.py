@@ -73,11 +73,27 @@ def test_weibel_full_size_fp32_split_per_result(weibel_full):
 
 
 def test_landau_full_1000_steps(oracle):
+    """Over 1000 steps the l = 7, 8 harmonics move by 2.5e-12 when f00 moves
+    by one ulp, and the C restatement itself differs from the reference's
+    own build by 2.3e-12 on l = 8 (measured on the CPU; the reference takes
+    ~9 minutes for this run): every harmonic is held to 1e-12 or, where the
+    problem's own rounding sensitivity is larger, to twice that sensitivity."""
     cfg, f, fields, _ = workloads.landau1d(0)
     st = State(deck_of(cfg), f, fields)
     ref = oracle.steps(st, 1000, 1)
+    bumped = st.copy()
+    bumped.f[0] *= 1.0 + 2.0 ** -52
+    sens = oracle.steps(bumped, 1000, 1)
     out = run_gpu(st, ["step:1000:1"], fast_path=True)
-    err, where = worst_rel(out, ref)
-    assert err <= TOL, (err, where)
+    top = max(float(np.linalg.norm(ref.harmonic(l, m))) for (l, m) in st.deck.harmonics())
+    for (l, m) in st.deck.harmonics():
+        den = max(float(np.linalg.norm(ref.harmonic(l, m))), 1e-9 * top)
+        s = float(np.linalg.norm(sens.harmonic(l, m) - ref.harmonic(l, m))) / den
+        e = float(np.linalg.norm(out.harmonic(l, m) - ref.harmonic(l, m))) / den
+        assert e <= max(TOL, 2.0 * s), ((l, m), e, s)
+    nE = float(np.linalg.norm(ref.fields[0]))
+    sE = float(np.linalg.norm(sens.fields[0] - ref.fields[0])) / nE
+    eE = float(np.linalg.norm(out.fields[0] - ref.fields[0])) / nE
+    assert eE <= max(TOL, 2.0 * sE), (eE, sE)
     # the damped field is still resolved: E_x carries the wave after 1000 steps
     assert np.linalg.norm(ref.fields[0]) > 0

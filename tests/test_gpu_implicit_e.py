@@ -7,9 +7,9 @@ The RK2 actions alone (advance_p1: advection + B + Faraday; advance_p2: the
 E couplings + CLEAN_LOW_PC) hold the FP64 bar of 1e-12.  The implicit E
 itself comes from finite differences of the plasma's current under probe
 fields of relative size sqrt(16 eps) = 6e-8, which amplify any rounding
-difference by ~1e7: the reference's own output moves by ~1e-8 when its input
-moves by one ulp.  The full step is held to a small multiple of that
-sensitivity, measured in the test on the same deck.
+difference by ~1e8: the reference's own output moves by ~3e-8 when every
+element of its input moves by one ulp.  The full step is held to a small
+multiple of that sensitivity, measured in the test on the same deck.
 """
 import numpy as np
 import pytest
@@ -19,7 +19,7 @@ from tests.gpu_util import cfg_of, worst_rel
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
-SENS_FACTOR = 100.0   # full step: within this many times the reference's 1-ulp sensitivity
+SENS_FACTOR = 10.0    # full step: within this many times the reference's 1-ulp sensitivity
 
 
 def _deck(one_d=False, **kw):
@@ -59,14 +59,21 @@ def test_rk2_actions_match_reference(mask, one_d):
     assert err <= TOL, (err, where)
 
 
+def ulp_noise(st, seed):
+    """the state with every element moved by one ulp, up or down at random"""
+    rng = np.random.default_rng(seed)
+    out = st.copy()
+    out.f = out.f * (1.0 + 2.0 ** -52 * rng.choice([-1.0, 1.0], size=out.f.shape))
+    return out
+
+
 @pytest.mark.parametrize("one_d", [False, True])
 def test_implicit_step_within_reference_sensitivity(one_d):
     d = _deck(one_d)
     st = _state(d, 72)
     ref = run_reference(st, ["istep:1:63"])
-    bumped = st.copy()
-    bumped.f[0] *= 1.0 + 2.0 ** -52
-    sens, _ = worst_rel(run_reference(bumped, ["istep:1:63"]), ref)
+    # the reference's own response to rounding-level changes of its input
+    sens = max(worst_rel(run_reference(ulp_noise(st, k), ["istep:1:63"]), ref)[0] for k in (1, 2))
     err, where = worst_rel(run_imp(st, 1, 63), ref)
     print(f"implicit step ({'1D' if one_d else '2D'}): error {err:.3e} at {where}, reference sensitivity {sens:.3e}")
     assert err <= max(SENS_FACTOR * sens, TOL), (err, where, sens)
