@@ -40,9 +40,10 @@ typedef enum oshun_status {
 
 typedef enum oshun_precision {
     OSHUN_FP64 = 0,       /* every operator in IEEE FP64: the drop-in */
-    OSHUN_FP32_SPLIT = 1  /* f_lm (l >= 1), fields and their arithmetic in FP32; f00, the
-                             Rosenbluth integrals, the collision solves and the current
-                             reduction in FP64 */
+    OSHUN_FP32_SPLIT = 1  /* f_lm (l >= 1), fields and their arithmetic in FP32 (the planes
+                             stored relative to an FP64 momentum profile, see
+                             oshun_plane_profile); f00, the Rosenbluth integrals, the
+                             collision solves and the current reduction in FP64 */
 } oshun_precision;
 
 /* flags */
@@ -168,6 +169,13 @@ int oshun_device_state(oshun_handle h, void** f00, void** planes, void** fields,
 /* Plane index of the real part of harmonic (l,m) in `planes` (the imaginary
  * part, m > 0, follows it), or -1 for (0,0), which lives in `f00`. */
 int oshun_plane_index(oshun_handle h, int l, int m, int* plane);
+/* OSHUN_FP32_SPLIT: the l >= 1 planes hold f minus a momentum profile per
+ * plane, the average over the cells of the state at its last upload
+ * (rounded to FP32), so that the x and y differences of a harmonic with a
+ * large, nearly uniform part act on its small deviation and FP32 storage
+ * keeps that deviation's precision.  *profile = the device array
+ * [nplanes][nump] (FP64 values), or NULL in OSHUN_FP64 and in batches. */
+int oshun_plane_profile(oshun_handle h, const double** profile);
 /* The configuration the handle was created with. */
 int oshun_get_config(oshun_handle h, oshun_cfg* cfg);
 

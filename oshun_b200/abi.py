@@ -33,7 +33,7 @@ EXPORTED = [
     "oshun_adjoint_create", "oshun_adjoint_destroy", "oshun_adjoint_set_stream", "oshun_adjoint_state_size",
     "oshun_adjoint_forward", "oshun_adjoint_vjp", "oshun_debug_inject_stage_timeout", "oshun_get_config",
     "oshun_moments", "oshun_restart_bytes", "oshun_restart_pack", "oshun_restart_unpack", "oshun_restart_write",
-    "oshun_restart_read", "oshun_rk2_imp_step",
+    "oshun_restart_read", "oshun_rk2_imp_step", "oshun_plane_profile",
 ]
 
 
@@ -90,6 +90,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_debug_inject_stage_timeout.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     lib.oshun_get_config.argtypes = [vp, ctypes.POINTER(OshunCfg)]
     lib.oshun_rk2_imp_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.oshun_plane_profile.argtypes = [vp, ctypes.POINTER(vp)]
     lib.oshun_moments.argtypes = [vp, vp]
     lib.oshun_restart_bytes.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int]
     lib.oshun_restart_bytes.restype = ctypes.c_longlong

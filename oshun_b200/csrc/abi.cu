@@ -80,7 +80,7 @@ struct Clock {
 template <typename TS>
 __global__ void scatter_kernel(const double2* __restrict__ src, double* f00, TS* planes, TS* fields,
                                const int* __restrict__ hplane, long long pstride, int nh, long long cells,
-                               int* flag) {
+                               int* flag, const double* __restrict__ ref, int np) {
     const long long total = (long long)nh * pstride + 6 * cells;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
@@ -93,10 +93,12 @@ __global__ void scatter_kernel(const double2* __restrict__ src, double* f00, TS*
                 f00[off] = v.x;
                 if (v.y != 0.0) *flag = 1;
             } else if (q >= 0 && hplane[nh + h]) {     // m > 0: Re, Im
-                planes[(long long)q * pstride + off] = (TS)v.x;
-                planes[(long long)(q + 1) * pstride + off] = (TS)v.y;
+                const int p = (int)(off % np);
+                planes[(long long)q * pstride + off] = (TS)(ref ? v.x - ref[(long long)q * np + p] : v.x);
+                planes[(long long)(q + 1) * pstride + off] = (TS)(ref ? v.y - ref[(long long)(q + 1) * np + p] : v.y);
             } else {
-                planes[(long long)q * pstride + off] = (TS)v.x;
+                const int p = (int)(off % np);
+                planes[(long long)q * pstride + off] = (TS)(ref ? v.x - ref[(long long)q * np + p] : v.x);
                 if (v.y != 0.0) *flag = 1;
             }
         } else {
@@ -109,7 +111,8 @@ __global__ void scatter_kernel(const double2* __restrict__ src, double* f00, TS*
 
 template <typename TS>
 __global__ void gather_kernel(double2* __restrict__ dst, const double* f00, const TS* planes, const TS* fields,
-                              const int* __restrict__ hplane, long long pstride, int nh, long long cells) {
+                              const int* __restrict__ hplane, long long pstride, int nh, long long cells,
+                              const double* __restrict__ ref, int np) {
     const long long total = (long long)nh * pstride + 6 * cells;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
@@ -118,14 +121,63 @@ __global__ void gather_kernel(double2* __restrict__ dst, const double* f00, cons
             const int h = (int)(i / pstride);
             const long long off = i - (long long)h * pstride;
             const int q = hplane[h];
+            const int p = (int)(off % np);
+            auto val = [&](long long qq) {
+                return (double)planes[qq * pstride + off] + (ref ? ref[qq * np + p] : 0.0);
+            };
             if (q < 0) v = make_double2(f00[off], 0.0);
-            else if (hplane[nh + h]) v = make_double2((double)planes[(long long)q * pstride + off],
-                                                      (double)planes[(long long)(q + 1) * pstride + off]);
-            else v = make_double2((double)planes[(long long)q * pstride + off], 0.0);
+            else if (hplane[nh + h]) v = make_double2(val(q), val(q + 1));
+            else v = make_double2(val(q), 0.0);
         } else {
             v = make_double2((double)fields[i - (long long)nh * pstride], 0.0);
         }
         dst[i] = v;
+    }
+}
+
+// FP32 split: the momentum profile each l >= 1 plane is stored relative to,
+// the average over the cells of the uploaded state.  Partial sums over
+// chunks of cells, then the chunks in order (deterministic); the profile is
+// rounded to the plane type so that the stored deviation and every reader
+// (stage, collision, moments, download) use one value.
+constexpr int kProfChunks = 64;
+__global__ void profile_partial_kernel(const double2* __restrict__ src, const int* __restrict__ hplane,
+                                       long long cells, int np, double2* part) {
+    const int h = blockIdx.x, ch = blockIdx.y;
+    if (hplane[h] < 0) return;   // f00 is FP64
+    const long long c0 = cells * ch / kProfChunks, c1 = cells * (ch + 1) / kProfChunks;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        double sr = 0.0, si = 0.0;
+        for (long long c = c0; c < c1; ++c) {
+            const double2 v = src[((long long)h * cells + c) * np + p];
+            sr += v.x;
+            si += v.y;
+        }
+        part[((long long)h * kProfChunks + ch) * np + p] = make_double2(sr, si);
+    }
+}
+template <typename TS>
+__global__ void profile_final_kernel(const double2* __restrict__ part, const int* __restrict__ hplane, int nh,
+                                     long long cells, int np, double* ref64, TS* refts) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)nh * np;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int h = (int)(i / np), p = (int)(i - (long long)h * np);
+        const int q = hplane[h];
+        if (q < 0) continue;
+        double sr = 0.0, si = 0.0;
+        for (int ch = 0; ch < kProfChunks; ++ch) {
+            const double2 v = part[((long long)h * kProfChunks + ch) * np + p];
+            sr += v.x;
+            si += v.y;
+        }
+        const TS r = (TS)(sr / (double)cells);
+        ref64[(long long)q * np + p] = (double)r;
+        refts[(long long)q * np + p] = r;
+        if (hplane[nh + h]) {
+            const TS ri = (TS)(si / (double)cells);
+            ref64[(long long)(q + 1) * np + p] = (double)ri;
+            refts[(long long)(q + 1) * np + p] = ri;
+        }
     }
 }
 
@@ -205,6 +257,12 @@ struct oshun_ctx {
     Clock* d_clock = nullptr;
     double2* d_stage = nullptr;  // host-layout staging for transfers and slopes
     std::vector<CoefLM> coef_host;   // the coupling table on the host
+    // FP32 split: the l >= 1 planes store f minus a momentum profile per plane
+    // (the cell average at upload), FP64 and plane-type copies [nplanes][np]
+    bool use_profile = false;
+    double* d_ref64 = nullptr;
+    void* d_ref_ts = nullptr;
+    double2* d_refpart = nullptr;
     // implicit electric field (built on first use): coupling tables of
     // ImpEx, ImpEx1D, ImpEy/z and Exyz1D; J0, J(DEx), J(DEy), J(DEz), JN, DE,
     // EN ([3][cells] each) and p^3/gamma; the probe field; the zero count
@@ -325,6 +383,7 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     StageArgs<TS> a;
     std::memset(&a, 0, sizeof(a));
     a.f00_in = f00[in_set]; a.pl_in = (const TS*)pl[in_set]; a.fld_in = (const TS*)fld[in_set];
+    a.pl_ref = use_profile ? (const TS*)d_ref_ts : nullptr;
     a.coef = d_coef; a.plane_of = d_plane_of;
     a.inv_pr = d_ptab; a.vr = d_ptab + cfg.nump; a.wj = d_ptab + 2 * cfg.nump;
     a.cells = cells; a.pstride = pstride;
@@ -556,6 +615,7 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     if (set < 0) set = h->cur;
     a.f00 = h->f00[set];
     a.planes = h->pl[set];
+    a.pl_ref = h->use_profile ? h->d_ref64 : nullptr;
     a.planes_fp32 = h->fp32 ? 1 : 0;
     a.plane_of = h->d_plane_of; a.plane_l = h->d_plane_l; a.plane_m = h->d_plane_m;
     a.nplanes = h->nplanes;
@@ -688,6 +748,7 @@ ImplicitArgs implicit_args(const oshun_ctx* h) {
     ImplicitArgs a;
     std::memset(&a, 0, sizeof(a));
     for (int i = 0; i < 4; ++i) a.planes[i] = h->pl[i];
+    a.pl_ref = h->use_profile ? h->d_ref64 : nullptr;
     a.cells = h->cells; a.pstride = h->pstride;
     a.np = c.nump; a.nx = c.numx; a.ny = c.numy;
     a.q10 = h->plane_of_host[(size_t)(c.m0 + 1)];
@@ -808,6 +869,7 @@ void free_ctx(oshun_ctx* h) {
     cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
     cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage); cudaFree(h->d_jw);
     cudaFree(h->d_mom_tab); cudaFree(h->d_mom);
+    cudaFree(h->d_ref64); cudaFree(h->d_ref_ts); cudaFree(h->d_refpart);
     for (int i = 0; i < 4; ++i) cudaFree(h->d_coef_imp[i]);
     cudaFree(h->d_imp); cudaFree(h->d_fe); cudaFree(h->d_zeros);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -866,6 +928,16 @@ int oshun_create(const oshun_cfg* cfg, oshun_handle* out) {
     CKF(cudaMemset(h->d_status, 0, sizeof(int) * 4));
     CKF(cudaMalloc(&h->d_jw, sizeof(double) * 24 * h->cells));
     CKF(cudaMemset(h->d_jw, 0, sizeof(double) * 24 * h->cells));
+    if (h->fp32) {
+        // the FP32 planes are stored relative to a momentum profile per plane
+        const size_t nr = (size_t)std::max(1, h->nplanes) * cfg->nump;
+        h->use_profile = true;
+        CKF(cudaMalloc(&h->d_ref64, sizeof(double) * nr));
+        CKF(cudaMemset(h->d_ref64, 0, sizeof(double) * nr));
+        CKF(cudaMalloc(&h->d_ref_ts, sizeof(float) * nr));
+        CKF(cudaMemset(h->d_ref_ts, 0, sizeof(float) * nr));
+        CKF(cudaMalloc(&h->d_refpart, sizeof(double2) * (size_t)h->nh * kProfChunks * cfg->nump));
+    }
     CKF(cudaMalloc(&h->d_clock, sizeof(Clock)));
     Clock ck{h->t, h->t_ee, h->t_eb};
     CKF(cudaMemcpy(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice));
@@ -942,14 +1014,23 @@ int oshun_upload(oshun_handle h, const double* harmonics, const double* fields) 
     CK(cudaMemsetAsync(h->d_status + 2, 0, sizeof(int), h->stream));
     const long long total = (long long)h->nh * h->pstride + 6 * h->cells;
     const int set = h->cur;
+    const int np = h->cfg.nump;
+    if (h->use_profile) {
+        profile_partial_kernel<<<dim3((unsigned)h->nh, kProfChunks), 128, 0, h->stream>>>(h->d_stage, h->d_hplane,
+                                                                                           h->cells, np, h->d_refpart);
+        profile_final_kernel<float><<<grid_for((long long)h->nh * np, 128), 128, 0, h->stream>>>(
+            h->d_refpart, h->d_hplane, h->nh, h->cells, np, h->d_ref64, (float*)h->d_ref_ts);
+        CK(cudaGetLastError());
+    }
+    const double* ref = h->use_profile ? h->d_ref64 : nullptr;
     if (h->fp32)
         scatter_kernel<float><<<grid_for(total, 256), 256, 0, h->stream>>>(
             h->d_stage, h->f00[set], (float*)h->pl[set], (float*)h->fld[set], h->d_hplane, h->pstride, h->nh,
-            h->cells, h->d_status + 2);
+            h->cells, h->d_status + 2, ref, np);
     else
         scatter_kernel<double><<<grid_for(total, 256), 256, 0, h->stream>>>(
             h->d_stage, h->f00[set], (double*)h->pl[set], (double*)h->fld[set], h->d_hplane, h->pstride, h->nh,
-            h->cells, h->d_status + 2);
+            h->cells, h->d_status + 2, ref, np);
     CK(cudaGetLastError());
     int flag = 0;
     CK(cudaMemcpyAsync(&flag, h->d_status + 2, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -958,16 +1039,19 @@ int oshun_upload(oshun_handle h, const double* harmonics, const double* fields) 
     return OSHUN_OK;
 }
 
-static int gather_to_host(oshun_handle h, int set, double* harmonics, double* fields) {
+// with_profile: the set holds a state (stored relative to the planes'
+// profile); a slope is gathered as it is
+static int gather_to_host(oshun_handle h, int set, double* harmonics, double* fields, bool with_profile = true) {
     const long long total = (long long)h->nh * h->pstride + 6 * h->cells;
+    const double* ref = (with_profile && h->use_profile) ? h->d_ref64 : nullptr;
     if (h->fp32)
         gather_kernel<float><<<grid_for(total, 256), 256, 0, h->stream>>>(
             h->d_stage, h->f00[set], (const float*)h->pl[set], (const float*)h->fld[set], h->d_hplane, h->pstride,
-            h->nh, h->cells);
+            h->nh, h->cells, ref, h->cfg.nump);
     else
         gather_kernel<double><<<grid_for(total, 256), 256, 0, h->stream>>>(
             h->d_stage, h->f00[set], (const double*)h->pl[set], (const double*)h->fld[set], h->d_hplane,
-            h->pstride, h->nh, h->cells);
+            h->pstride, h->nh, h->cells, ref, h->cfg.nump);
     CK(cudaGetLastError());
     const size_t nb_h = sizeof(double2) * (size_t)h->nh * h->pstride;
     const size_t nb_f = sizeof(double2) * 6 * (size_t)h->cells;
@@ -987,7 +1071,7 @@ int oshun_rhs(oshun_handle h, double* slope_harmonics, double* slope_fields) {
     // slope written to set 2 (scratch), in plane layout
     int rc = launch_stage(h, h->cur, h->cur, h->cur, 2, 1, 0, 1.0, 1.0);
     if (rc) return rc;
-    return gather_to_host(h, 2, slope_harmonics, slope_fields);
+    return gather_to_host(h, 2, slope_harmonics, slope_fields, false);
 }
 
 int oshun_rk4_step(oshun_handle h) {
@@ -1133,6 +1217,12 @@ int oshun_rk2_imp_step(oshun_handle h, int nsteps, int mask) {
     return OSHUN_OK;
 }
 
+int oshun_plane_profile(oshun_handle h, const double** profile) {
+    if (!h || !profile) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
+    *profile = h->use_profile ? h->d_ref64 : nullptr;
+    return OSHUN_OK;
+}
+
 int oshun_get_config(oshun_handle h, oshun_cfg* cfg) {
     if (!h || !cfg) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
     *cfg = h->cfg;
@@ -1166,6 +1256,7 @@ int oshun_moments(oshun_handle h, float* out) {
     std::memset(&a, 0, sizeof(a));
     a.f00 = h->f00[h->cur];
     a.planes = h->pl[h->cur];
+    a.pl_ref = h->use_profile ? h->d_ref64 : nullptr;
     a.cells = h->cells; a.pstride = h->pstride;
     a.np = np; a.nx = c.numx; a.ny = c.numy;
     auto plane = [&](int l, int m) {
@@ -1533,6 +1624,7 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
         oshun_handle h = nullptr;
         int rc = oshun_create(&c, &h);
         if (rc) return fail(rc);
+        h->use_profile = false;   // the batched kernels read the planes as they are stored
         b->P.push_back(h);
         b->collide.push_back(col);
         if ((rc = oshun_set_stream(h, b->stream))) return fail(rc);

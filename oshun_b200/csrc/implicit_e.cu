@@ -29,19 +29,22 @@ __global__ void implicit_current_kernel(const ImplicitArgs a, const int set, dou
     const int n = a.np;
     const double* w = a.p3og;
     const TP* pl = reinterpret_cast<const TP*>(a.planes[set]);
-    auto row_sum = [&](const TP* f) {
-        double s = (double)f[0] * w[0];
-        s = s + (double)f[n - 1] * w[n - 1];
-        for (int i = 1; i < n - 1; ++i) s = s + (double)f[i] * w[i];
+    // f of plane q at momentum point i: the stored value plus the plane's profile, if any
+    auto row_sum = [&](const int q) {
+        const TP* g = pl + (long long)q * a.pstride + cell * n;
+        const double* r = a.pl_ref ? a.pl_ref + (long long)q * n : nullptr;
+        auto f = [&](int i) { return (double)g[i] + (r ? r[i] : 0.0); };
+        double s = f(0) * w[0];
+        s = s + f(n - 1) * w[n - 1];
+        for (int i = 1; i < n - 1; ++i) s = s + f(i) * w[i];
         s = s * a.dp;
-        s = s + a.small * ((double)f[1] * w[1]);
+        s = s + a.small * (f(1) * w[1]);
         return s;
     };
-    const long long off = cell * n;
-    J[cell] = row_sum(pl + (long long)a.q10 * a.pstride + off) * a.c4;
+    J[cell] = row_sum(a.q10) * a.c4;
     if (a.q11 >= 0) {
-        const double re = row_sum(pl + (long long)a.q11 * a.pstride + off) * a.c8;
-        const double im = row_sum(pl + (long long)(a.q11 + 1) * a.pstride + off) * a.c8;
+        const double re = row_sum(a.q11) * a.c8;
+        const double im = row_sum(a.q11 + 1) * a.c8;
         J[a.cells + cell] = re;
         J[2 * a.cells + cell] = -im;
     } else {

@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(32 * kMomWarps) moments_cell_kernel(const Mome
             double v = 0.0;
             if (c < nc && which != -2) {
                 const long long i = (cell0 + c) * n + p;
-                v = which == -1 ? a.f00[i] : plane_at<TP>(a.planes, which, a.pstride, i);
+                v = which == -1 ? a.f00[i]
+                                : plane_at<TP>(a.planes, which, a.pstride, i) + (a.pl_ref ? a.pl_ref[(long long)which * n + p] : 0.0);
             }
             rows[c * ld + p] = v;
         }

@@ -56,6 +56,9 @@ enum : int {
 template <typename TS>
 struct StageArgs {
     const double* f00_in; const TS* pl_in; const TS* fld_in;   // stage input (F is evaluated here)
+    // FP32 split: the l >= 1 planes store f minus this momentum profile of
+    // each plane ([nplanes][np]); null: the planes store f
+    const TS* pl_ref;
     const double* f00_B;  const TS* pl_B;  const TS* fld_B;    // step base Y0
     double* f00_A;        TS* pl_A;        TS* fld_A;          // RK accumulator Y
     double* f00_out;      TS* pl_out;      TS* fld_out;        // next stage input (or the slope)
@@ -88,6 +91,7 @@ struct CollideArgs {
     double* f00;          // FP64 f00 plane (in/out)
     void* planes;         // l >= 1 planes (double or float)
     int planes_fp32;
+    const double* pl_ref; // [nplanes][np] momentum profile the planes are stored relative to (null: none)
     const int* plane_of;  // [(l0+1)*(m0+1)]
     const int* plane_l;   // [nplanes]: l of each plane
     const int* plane_m;   // [nplanes]: m of each plane
@@ -188,6 +192,7 @@ enum { kMomN = 0, kMomVx, kMomVy, kMomVxVx, kMomVyVy, kMomVzVz, kMomVxVy, kMomVx
 struct MomentArgs {
     const double* f00;    // FP64 f00 plane
     const void* planes;   // l >= 1 planes (double or float)
+    const double* pl_ref; // [nplanes][np] momentum profile the planes are stored relative to (null: none)
     long long cells, pstride;
     int np, nx, ny;
     int q10, q11, q20, q21, q22;   // plane of Re f_lm, -2 when the harmonic is absent
@@ -206,6 +211,7 @@ cudaError_t launch_moments(const MomentArgs& a, int planes_fp32, cudaStream_t s)
 // collision kernels
 struct ImplicitArgs {
     const void* planes[4];   // l >= 1 planes of each state set (double or float)
+    const double* pl_ref;    // [nplanes][np] momentum profile the planes are stored relative to (null: none)
     long long cells, pstride;
     int np, nx, ny;
     int q10, q11;            // planes of f10 and Re f11 (-1: absent)

@@ -224,6 +224,9 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         nb.xp = (cc + 2) * np + pc;
         nb.ym = has_y ? (tx + 2 + cc) * np + pc : nb.ctr;
         nb.yp = has_y ? (2 * tx + 2 + cc) * np + pc : nb.ctr;
+        nb.p = pc;
+        nb.p_m = pc - (pc > 0 ? 1 : 0);
+        nb.p_p = pc + (pc < np - 1 ? 1 : 0);
         const int roff = cc * np + pc;          // this point inside a staged row
 
         Th<TS> th;
@@ -318,14 +321,19 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * L.slot_bytes);
-                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th);
+                    const TS* ref = a.pl_ref ? a.pl_ref + (long long)splane[s * mstride + m] * np : nullptr;
+                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, ref, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
+                            // the current of f = ref + stored deviation
+                            const double r0 = a.pl_ref ? (double)a.pl_ref[(long long)splane[s * mstride + m] * np + pc] : 0.0;
                             if constexpr (m == 0) {
-                                jx += wj * (double)sb[nb.ctr];
+                                jx += wj * ((double)sb[nb.ctr] + r0);
                             } else {
-                                jyr += wj * (double)sb[nb.ctr];
-                                jyi += wj * (double)sb[seg + nb.ctr];
+                                const double r1 =
+                                    a.pl_ref ? (double)a.pl_ref[((long long)splane[s * mstride + m] + 1) * np + pc] : 0.0;
+                                jyr += wj * ((double)sb[nb.ctr] + r0);
+                                jyi += wj * ((double)sb[seg + nb.ctr] + r1);
                             }
                         }
                     }

@@ -154,6 +154,7 @@ __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, boo
 // per-thread element offsets of the stencil operands inside a slot
 struct Nb {
     int ctr, pm, pp, xm, xp, ym, yp;
+    int p, p_m, p_p;   // momentum index of the point and of its p-1, p+1 operands (edge rules applied)
 };
 
 // per-thread constants of the coupling arithmetic
@@ -313,7 +314,8 @@ __device__ __forceinline__ void couple_f00_row(TS (&R2)[MC + 1], TS (&I2)[MC + 1
 template <int MC, int M>
 __device__ __forceinline__ void couple_src3(AccD<MC>& A0, AccD<MC>& A1, AccD<MC>& A2, const CoefT<double>& c,
                                             const double* __restrict__ sb, const int seg, const Nb& nb,
-                                            const Th<double>& th) {
+                                            const Th<double>& th, const double* /*ref: FP64 planes hold f*/,
+                                            const int /*np*/) {
     couple_src3_ri<MC, M, double>(A0.R, A1.R, A2.R, A0.I, A1.I, A2.I, c, sb, seg, nb, th);
 }
 template <int MC>
@@ -329,10 +331,13 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 // FP32: the same couplings on (Re, Im) pairs.  With F = (fr, fi) and
 // F' = (fi, -fr), a complex coupling (a + i b) F adds a F + b F'; the
 // m = 0 sources (M = 0) carry Im = 0.
+// The planes hold f - ref (ref: the plane's momentum profile, null for
+// none): the x and y differences act on the stored deviation alone, the
+// momentum stencil and the value itself on f = ref + deviation.
 template <int MC, int M>
 __device__ __forceinline__ void couple_src3(AccF<MC>& A0, AccF<MC>& A1, AccF<MC>& A2, const CoefT<float>& c,
                                             const float* __restrict__ sb, const int seg, const Nb& nb,
-                                            const Th<float>& th) {
+                                            const Th<float>& th, const float* __restrict__ ref, const int np) {
     constexpr bool UP = M + 1 <= MC;
     constexpr bool DN = M >= 1;
     const float2 m1 = bc2(-1.f);
@@ -346,6 +351,12 @@ __device__ __forceinline__ void couple_src3(AccF<MC>& A0, AccF<MC>& A1, AccF<MC>
         xm.y = si[nb.xm]; xp.y = si[nb.xp]; ym.y = si[nb.ym]; yp.y = si[nb.yp];
     } else {
         f.y = 0.f; fm.y = 0.f; fp.y = 0.f; xm.y = 0.f; xp.y = 0.f; ym.y = 0.f; yp.y = 0.f;
+    }
+    if (ref) {
+        f.x += __ldg(ref + nb.p); fm.x += __ldg(ref + nb.p_m); fp.x += __ldg(ref + nb.p_p);
+        if constexpr (DN) {
+            f.y += __ldg(ref + np + nb.p); fm.y += __ldg(ref + np + nb.p_m); fp.y += __ldg(ref + np + nb.p_p);
+        }
     }
     const float2 dx = __fmul2_rn(fma2(xp, m1, xm), vr);   // (f(x-1) - f(x+1)) v
     const float2 dy = __fmul2_rn(fma2(yp, m1, ym), vr);
@@ -733,6 +744,9 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
         nb.xp = (cc + 2) * np + pc;
         nb.ym = has_y ? (tx + 2 + cc) * np + pc : nb.ctr;
         nb.yp = has_y ? (2 * tx + 2 + cc) * np + pc : nb.ctr;
+        nb.p = pc;
+        nb.p_m = pc - (pc > 0 ? 1 : 0);
+        nb.p_p = pc + (pc < np - 1 ? 1 : 0);
         const int seg = seg_cells * np;
         const int rstride = tx * np;            // plane stride inside a staged row
         const int roff = cc * np + pc;          // this point inside a staged row
@@ -814,7 +828,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th);
+                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, (const TS*)nullptr, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             if constexpr (m == 0) {

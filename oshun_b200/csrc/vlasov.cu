@@ -164,18 +164,26 @@ __global__ void __launch_bounds__(256) rk_stage_kernel(const StageArgs<TS> a) {
                     if (s == 0) return (TS)ld(a.f00_in + off);
                     return ld(src + comp * a.pstride + off);
                 };
-                TS fr = pv ? load(o, 0) : TS(0);
-                TS fi = (m > 0 && pv) ? load(o, 1) : TS(0);
+                // f itself (the stored value plus the plane's momentum profile, if any) at momentum
+                // index pp of this cell; the x and y differences below act on the stored values alone
+                const TS* ref = (s > 0 && a.pl_ref) ? a.pl_ref + (long long)ld(a.plane_of + s * mstride + m) * np
+                                                    : nullptr;
+                auto loadf = [&](long long off, int comp, int pp) -> TS {
+                    const TS v = load(off, comp);
+                    return ref ? v + ld(ref + comp * np + pp) : v;
+                };
+                TS fr = pv ? loadf(o, 0, p) : TS(0);
+                TS fi = (m > 0 && pv) ? loadf(o, 1, p) : TS(0);
                 TS frm = __shfl_up_sync(kFull, fr, 1), frp = __shfl_down_sync(kFull, fr, 1);
                 TS fim = TS(0), fip = TS(0);
                 if (m > 0) { fim = __shfl_up_sync(kFull, fi, 1); fip = __shfl_down_sync(kFull, fi, 1); }
                 if (pv && lane == 0 && p > 0) {
-                    frm = load(o - 1, 0);
-                    if (m > 0) fim = load(o - 1, 1);
+                    frm = loadf(o - 1, 0, p - 1);
+                    if (m > 0) fim = loadf(o - 1, 1, p - 1);
                 }
                 if (pv && lane == 31 && p + 1 < np) {
-                    frp = load(o + 1, 0);
-                    if (m > 0) fip = load(o + 1, 1);
+                    frp = loadf(o + 1, 0, p + 1);
+                    if (m > 0) fip = loadf(o + 1, 1, p + 1);
                 }
                 const TS dxr = pv ? (load(oxm, 0) - load(oxp, 0)) * vr : TS(0);
                 const TS dxi = (m > 0 && pv) ? (load(oxm, 1) - load(oxp, 1)) * vr : TS(0);
