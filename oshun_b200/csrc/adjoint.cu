@@ -8,7 +8,10 @@
 //   collide_adj_kernel the collision step's transpose, one thread per cell
 //                      (reverse sweep through the e-e RK4 substeps, the
 //                      transposed Thomas solves and the dependence of the
-//                      tridiagonal coefficients on f00), work space per cell
+//                      tridiagonal coefficients on f00), one cell a CTA with
+//                      its work space in shared memory where it fits (the
+//                      sweep is a long serial chain of work-space accesses:
+//                      shared memory instead of L2 shortens every link), else
 //                      in global memory;
 //   rk_combine_kernel  the linear combinations of the RK4 transpose.
 // State vectors use the plane layout: f00 plane, the l >= 1 planes, the 6
@@ -51,13 +54,16 @@ __global__ void stage_vjp_kernel(const Grid1 g, const double* __restrict__ s, co
 
 __global__ void collide_adj_kernel(const CollTables T, const int l0, const int nx, const double* __restrict__ y,
                                    double* __restrict__ lam, const int ee, const int eb, const int nsub,
-                                   const double hsub, const double Dt, double* __restrict__ ws, const long long wsz) {
+                                   const double hsub, const double Dt, double* __restrict__ ws, const long long wsz,
+                                   const int smem_ws) {
+    extern __shared__ double sws[];
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= nx) return;
     const int np = T.np;
     const long long pstride = (long long)nx * np;
+    double* w = smem_ws ? sws : ws + x * wsz;   // smem_ws: one thread a CTA
     adj::collide_cell_T(T, l0, y + (long long)x * np, y + pstride + (long long)x * np, pstride, ee, eb, nsub, hsub,
-                        Dt, lam + (long long)x * np, lam + pstride + (long long)x * np, pstride, ws + x * wsz);
+                        Dt, lam + (long long)x * np, lam + pstride + (long long)x * np, pstride, w);
 }
 
 // out = a0 * v0 + a1 * v1 (+ a2 * v2)
@@ -81,7 +87,14 @@ cudaError_t launch_stage_vjp(const Grid1& g, const double* s, const double* c, d
 
 cudaError_t launch_collide_adj(const CollTables& T, int l0, int nx, const double* y, double* lam, int ee, int eb,
                                int nsub, double hsub, double Dt, double* ws, long long wsz, cudaStream_t st) {
-    collide_adj_kernel<<<(nx + 63) / 64, 64, 0, st>>>(T, l0, nx, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz);
+    const size_t smem = sizeof(double) * (size_t)wsz;
+    if (smem <= 200 * 1024) {
+        const cudaError_t e = ensure_dyn_smem((const void*)collide_adj_kernel, smem);
+        if (e != cudaSuccess) return e;
+        collide_adj_kernel<<<nx, 1, smem, st>>>(T, l0, nx, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz, 1);
+    } else {
+        collide_adj_kernel<<<(nx + 63) / 64, 64, 0, st>>>(T, l0, nx, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz, 0);
+    }
     return cudaGetLastError();
 }
 
