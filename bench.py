@@ -395,23 +395,30 @@ def stage_roofline(h, stream, acct: dict, nrk: int, kernel: str, traffic=None) -
             "algorithmic_bytes_per_launch": acct["stage_bytes"], "avg_launch_ms": round(launch_ms, 4)}
 
 
-def rel_errors(a_f, a_fl, b_f, b_fl):
-    """max over harmonics and fields of the unfloored relative L2 error of a
-    against b, and where it is"""
+def rel_errors(a_f, a_fl, b_f, b_fl, floor: float = 1e-6):
+    """Error of the state a against the state b: the max over harmonics and
+    fields of the relative L2 error, each norm floored at `floor` times the
+    largest harmonic (or field) norm, so that a harmonic that is zero up to
+    rounding in b is measured against the state's own scale; and the relative
+    L2 error of the whole distribution.  Returns (worst, where, state)."""
     worst, where = 0.0, None
+    topf = max(float(np.linalg.norm(b_f[i])) for i in range(b_f.shape[0]))
+    topl = max(float(np.linalg.norm(b_fl[i])) for i in range(6))
     for i in range(b_f.shape[0]):
-        nb = float(np.linalg.norm(b_f[i]))
+        nb = max(float(np.linalg.norm(b_f[i])), floor * topf)
         if nb > 0:
             e = float(np.linalg.norm(a_f[i] - b_f[i])) / nb
             if e > worst:
                 worst, where = e, f"harmonic {i}"
     for i in range(6):
-        nb = float(np.linalg.norm(b_fl[i]))
+        nb = max(float(np.linalg.norm(b_fl[i])), floor * topl)
         if nb > 0:
             e = float(np.linalg.norm(a_fl[i] - b_fl[i])) / nb
             if e > worst:
                 worst, where = e, f"field {i}"
-    return worst, where
+    nf = float(np.linalg.norm(b_f))
+    state = float(np.linalg.norm(a_f - b_f)) / nf if nf > 0 else 0.0
+    return worst, where, state
 
 
 def form_single(workload: str, prec: int, steps: int, warmup: int, stream, err_steps: int = 2) -> dict:
@@ -444,9 +451,11 @@ def form_single(workload: str, prec: int, steps: int, warmup: int, stream, err_s
                 h.step(err_steps, collisions=col)
             fa, fla = a.download()
             fb, flb = b.download()
-        e, where = rel_errors(fb, flb, fa, fla)
+        e, where, st = rel_errors(fb, flb, fa, fla)
         out["max_rel_err_vs_fp64"] = e
         out["max_rel_err_at"] = where
+        out["state_rel_err_vs_fp64"] = st
+        out["err_norm_floor"] = "1e-6 of the largest harmonic / field norm"
         out["err_steps"] = err_steps
     return out
 
@@ -697,7 +706,7 @@ def measure_batch(n: int, prec: int, steps: int, warmup: int, stream, local: int
         for i, (_, f, fl, _) in enumerate(probs):
             b.upload(i, f, fl)
         b.step(2)
-        worst, where = 0.0, None
+        worst, where, wstate = 0.0, None, 0.0
         for i in pick:
             cfg, f, fl, col = probs[i]
             fb, flb = b.download(i)
@@ -706,11 +715,14 @@ def measure_batch(n: int, prec: int, steps: int, warmup: int, stream, local: int
                 h.upload(f, fl)
                 h.step(2, collisions=bool(col))
                 fa, fla = h.download()
-            e, w = rel_errors(fb, flb, fa, fla)
+            e, w, st = rel_errors(fb, flb, fa, fla)
+            wstate = max(wstate, st)
             if e > worst:
                 worst, where = e, f"problem {i}, {w}"
         out["max_rel_err_vs_fp64"] = worst
         out["max_rel_err_at"] = where
+        out["state_rel_err_vs_fp64"] = wstate
+        out["err_norm_floor"] = "1e-6 of the largest harmonic / field norm"
         out["err_steps"] = 2
         out["err_sample"] = f"problems {pick}"
     b.close()

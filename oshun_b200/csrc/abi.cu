@@ -1624,7 +1624,6 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
         oshun_handle h = nullptr;
         int rc = oshun_create(&c, &h);
         if (rc) return fail(rc);
-        h->use_profile = false;   // the batched kernels read the planes as they are stored
         b->P.push_back(h);
         b->collide.push_back(col);
         if ((rc = oshun_set_stream(h, b->stream))) return fail(rc);

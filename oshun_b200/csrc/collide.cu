@@ -39,10 +39,10 @@ constexpr int kCollideThreads = 128;
 // inside the lane's own run), the lanes' run totals are combined by a warp
 // scan, and the lane then accumulates its run again from the scanned start
 // out of the kept terms; the three chains are independent and interleaved.
-template <int G = 32, class T4, class T2, class T1>
+template <class T4, class T2, class T1>
 __device__ void warp_cumsum3(double* I4, double* I2, double* J1, int n, T4 t4, T2 t2, T1 t1) {
-    const int lane = threadIdx.x & (G - 1);   // lane in the group of G lanes owning this cell
-    const int E = (n + G - 1) / G;
+    const int lane = threadIdx.x & 31;
+    const int E = (n + 31) >> 5;
     const int b = min(lane * E, n), e = min(b + E, n);
     double l4 = 0.0, l2 = 0.0, l1 = 0.0;
     for (int k = b; k < e; ++k) {
@@ -59,17 +59,17 @@ __device__ void warp_cumsum3(double* I4, double* I2, double* J1, int n, T4 t4, T
     }
     double s4 = l4, s2 = l2, s1 = l1;
 #pragma unroll
-    for (int off = 1; off < G; off <<= 1) {
-        const double v4 = __shfl_up_sync(kFull, s4, off, G);
-        const double v2 = __shfl_up_sync(kFull, s2, off, G);
-        const double v1 = __shfl_down_sync(kFull, s1, off, G);
+    for (int off = 1; off < 32; off <<= 1) {
+        const double v4 = __shfl_up_sync(kFull, s4, off);
+        const double v2 = __shfl_up_sync(kFull, s2, off);
+        const double v1 = __shfl_down_sync(kFull, s1, off);
         if (lane >= off) { s4 += v4; s2 += v2; }
-        if (lane + off < G) s1 += v1;
+        if (lane + off < 32) s1 += v1;
     }
-    double r4 = __shfl_up_sync(kFull, s4, 1, G), r2 = __shfl_up_sync(kFull, s2, 1, G);
-    double r1 = __shfl_down_sync(kFull, s1, 1, G);
+    double r4 = __shfl_up_sync(kFull, s4, 1), r2 = __shfl_up_sync(kFull, s2, 1);
+    double r1 = __shfl_down_sync(kFull, s1, 1);
     if (lane == 0) { r4 = 0.0; r2 = 0.0; }
-    if (lane == G - 1) r1 = 0.0;
+    if (lane == 31) r1 = 0.0;
     for (int k = b; k < e; ++k) {
         if (k > 0) { r4 += I4[k]; r2 += I2[k]; }
         I4[k] = r4;
@@ -155,18 +155,17 @@ __device__ __forceinline__ StepP step_params(const CollideArgs& a) {
 }
 
 // EE_isotropic_conserva::Getslope on warp 0: fh = C_ee(fin)
-template <int G = 32>
 __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin, double* fh) {
     const int n = a.np;
-    const int lane = threadIdx.x & (G - 1);
-    warp_cumsum3<G>(s.I4, s.I2, s.J1, n, [&](int k) { return a.U4[k] * fin[k] + a.U4m1[k] * fin[k - 1]; },
+    const int lane = threadIdx.x & 31;
+    warp_cumsum3(s.I4, s.I2, s.J1, n, [&](int k) { return a.U4[k] * fin[k] + a.U4m1[k] * fin[k - 1]; },
                  [&](int k) { return a.U2[k] * fin[k] + a.U2m1[k] * fin[k - 1]; },
                  [&](int i) { return a.U1[i] * fin[i] + a.U1m1[i] * fin[i - 1]; });
     const double lnee = log_ee(4.0 * M_PI * s.I2[n - 1], 4.0 * M_PI * s.I4[n - 1], a.density_np);
     const double* vr = a.vr;
     const double v0s = vr[0] * vr[0], v1s = vr[1] * vr[1];
     // flux G_n (stored in I4); the first NB cells use the parabolic fit near v = 0
-    for (int k = lane; k < n; k += G) {
+    for (int k = lane; k < n; k += 32) {
         double g;
         if (k < a.NB) {
             const double f00 = (fin[0] - fin[1] * v0s / v1s) / (1.0 - v0s / v1s);
@@ -186,10 +185,10 @@ __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin,
     }
     __syncwarp();
     // D_k = (G_k - G_{k+1}) P_k for k < n-1, D_{n-1} = G_{n-1}   (kept in I2)
-    for (int k = lane; k < n; k += G) s.I2[k] = (k < n - 1) ? (s.I4[k] - s.I4[k + 1]) * a.Pn[k] : s.I4[k];
+    for (int k = lane; k < n; k += 32) s.I2[k] = (k < n - 1) ? (s.I4[k] - s.I4[k + 1]) * a.Pn[k] : s.I4[k];
     __syncwarp();
     const double norm = a.c_kpre * lnee;
-    for (int k = lane; k < n; k += G) {
+    for (int k = lane; k < n; k += 32) {
         double v;
         if (k == 0) {
             v = (-1.0) * s.I4[0];
@@ -205,16 +204,15 @@ __device__ void ee_slope(const CollideArgs& a, const Smem& s, const double* fin,
 }
 
 // Implicit_FLM_step::reset_coeff on warp 0 (f = f00 of the cell in smem)
-template <int G = 32>
 __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) {
     const StepP sp = step_params(a);
     const int n = a.np;
-    const int lane = threadIdx.x & (G - 1);
+    const int lane = threadIdx.x & 31;
     const double* vr = a.vr;
     double* I2 = s.I4;   // reuse the e-e work arrays
     double* I0 = s.I2;
     double* J1m = s.J1;
-    warp_cumsum3<G>(I2, I0, J1m, n, [&](int k) { return a.U4[k] * f[k] + a.U4m1[k] * f[k - 1]; },
+    warp_cumsum3(I2, I0, J1m, n, [&](int k) { return a.U4[k] * f[k] + a.U4m1[k] * f[k - 1]; },
                  [&](int k) { return a.U2[k] * f[k] + a.U2m1[k] * f[k - 1]; },
                  [&](int i) { return a.U1[i] * f[i] + a.U1m1[i] * f[i - 1]; });
     const double I2_temperature = I2[n - 1] * (4.0 * M_PI);
@@ -223,7 +221,7 @@ __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) 
     const double zlnei = zlog_ei(I0_density, I2_temperature, a.density_np, a.Zeta);
     const double scale = (-1.0) * lnee * a.kpre * sp.Dt;
     if (lane == 0) s.sc[0] = scale;
-    for (int k = lane; k < n; k += G) {
+    for (int k = lane; k < n; k += 32) {
         double i2 = I2[k] * (4.0 * M_PI);
         i2 /= vr[k] * vr[k];
         const double i0 = I0[k] * (4.0 * M_PI);
@@ -251,7 +249,7 @@ __device__ void flm_reset(const CollideArgs& a, const Smem& s, const double* f) 
         s.f0[k] = (k >= 1) ? (f[k - 1] - f[k]) / (vr[k] - vr[k - 1]) : 0.0;
     }
     __syncwarp();
-    for (int k = lane; k < n; k += G) {
+    for (int k = lane; k < n; k += 32) {
         double df, ddf;
         if (k == 0) {
             const double f00 = (f[0] - (vr[0] * vr[0] / (vr[1] * vr[1])) * f[1]) / (1.0 - (vr[0] * vr[0]) / (vr[1] * vr[1]));
@@ -474,36 +472,35 @@ __device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell
 }
 
 // e-e RK4 substeps of Explicit_EC_FP::loop on one warp (f00 of the cell in s.f)
-template <int G = 32>
 __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
     const StepP sp = step_params(a);
     const int n = a.np;
-    const int lane = threadIdx.x & (G - 1);
+    const int lane = threadIdx.x & 31;
     for (int sub = 0; sub < sp.nsub; ++sub) {
         const double h = sp.hsub;
-        for (int k = lane; k < n; k += G) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
+        for (int k = lane; k < n; k += 32) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
         __syncwarp();
-        ee_slope<G>(a, s, s.f1, s.fh);
-        for (int k = lane; k < n; k += G) {
+        ee_slope(a, s, s.f1, s.fh);
+        for (int k = lane; k < n; k += 32) {
             double t = s.fh[k] * (0.5 * h);
             s.f1[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
         }
         __syncwarp();
-        ee_slope<G>(a, s, s.f1, s.fh);
-        for (int k = lane; k < n; k += G) {
+        ee_slope(a, s, s.f1, s.fh);
+        for (int k = lane; k < n; k += 32) {
             s.f1[k] = s.f0[k];
             double t = s.fh[k] * (0.5 * h);
             s.f1[k] += t; t *= 2.0 / 3.0; s.f[k] += t;
         }
         __syncwarp();
-        ee_slope<G>(a, s, s.f1, s.fh);
-        for (int k = lane; k < n; k += G) {
+        ee_slope(a, s, s.f1, s.fh);
+        for (int k = lane; k < n; k += 32) {
             double t = s.fh[k] * h;
             s.f0[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
         }
         __syncwarp();
-        ee_slope<G>(a, s, s.f0, s.fh);
-        for (int k = lane; k < n; k += G) s.f[k] += s.fh[k] * (h / 6.0);
+        ee_slope(a, s, s.f0, s.fh);
+        for (int k = lane; k < n; k += 32) s.f[k] += s.fh[k] * (h / 6.0);
         __syncwarp();
     }
 }
@@ -691,17 +688,11 @@ __host__ __device__ inline size_t lane_smem_doubles(int np, int l0) {
     return 4 + 4 * (size_t)np + (work > piv ? work : piv);
 }
 
-// G: lanes per cell (32, or 16 with two cells a warp, each half its own
-// shared-memory work space); `valid` false: the lanes compute alongside the
-// other half of the warp (whose shuffles they join) but store nothing.
-template <typename TP, int E, int P, int G = 32>
-__device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const long long cell, double* smem,
-                                                  const bool valid = true) {
-    static_assert(G == 16 || G == 32, "cells own 16 or 32 lanes");
-    constexpr int LG = G == 32 ? 5 : 4;   // scan steps
+template <typename TP, int E, int P>
+__device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const long long cell, double* smem) {
     const int n = a.np;
     const int l0 = a.l0;
-    const int lane = threadIdx.x & (G - 1);
+    const int lane = threadIdx.x & 31;
     TP* planes = reinterpret_cast<TP*>(a.planes);
     const bool solve = a.do_l1 || a.do_lm;
     const Smem s = carve_lane(smem, n);
@@ -738,17 +729,16 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
         int bl, bj;
         batch_first(bl, bj);
         if (solve) load_batch(cell, bl, bj, cur);   // in flight during the e-e step
-        for (int k = lane; k < n; k += G) s.f[k] = a.f00[cell * n + k];
+        for (int k = lane; k < n; k += 32) s.f[k] = a.f00[cell * n + k];
         __syncwarp();
         if (a.do_ee) {
-            ee_substeps<G>(a, s);
-            if (valid)
-                for (int k = lane; k < n; k += G) a.f00[cell * n + k] = s.f[k];
+            ee_substeps(a, s);
+            for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
         }
         if (!solve) return;
-        flm_reset<G>(a, s, s.f);
+        flm_reset(a, s, s.f);
         // pivots of every collided l, one lane per l
-        for (int l = 1 + lane; l <= l0; l += G) {
+        for (int l = 1 + lane; l <= l0; l += 32) {
             if (!collided(a, l, 0)) continue;
             const double ll1 = l * ((-0.5) * (l + 1.0));
             double* cpl = piv + (size_t)(l - 1) * 2 * n;
@@ -772,7 +762,7 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
         for (int e = 0; e < E; ++e) ta[e] = (i0 + e < n) ? s.tri_a[i0 + e] : 0.0;
 
         int cl = -1;   // l of the per-l constants below
-        double id[E], cp[E], Af[LG], Ab[LG];
+        double id[E], cp[E], Af[5], Ab[5];
         while (bl <= l0) {
             const int l = bl, j = bl <= l0 ? bj : 0;
             const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
@@ -798,13 +788,13 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
                     if (i < n) B = (i == n - 1) ? 0.0 : B * (-cp[e]);
                 }
 #pragma unroll
-                for (int k = 0, off = 1; k < LG; ++k, off <<= 1) {
+                for (int k = 0, off = 1; k < 5; ++k, off <<= 1) {
                     Af[k] = A;
                     Ab[k] = B;
-                    const double Ap = __shfl_up_sync(kFull, A, off, G);
-                    const double Bp = __shfl_down_sync(kFull, B, off, G);
+                    const double Ap = __shfl_up_sync(kFull, A, off);
+                    const double Bp = __shfl_down_sync(kFull, B, off);
                     if (lane >= off) A *= Ap;
-                    if (lane + off < G) B *= Bp;
+                    if (lane + off < 32) B *= Bp;
                 }
             }
             // forward: run offsets, scan, recursion inside the run
@@ -820,16 +810,16 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
                 Bf[b] = B;
             }
 #pragma unroll
-            for (int k = 0, off = 1; k < LG; ++k, off <<= 1) {
+            for (int k = 0, off = 1; k < 5; ++k, off <<= 1) {
 #pragma unroll
                 for (int b = 0; b < P; ++b) {
-                    const double Bp = __shfl_up_sync(kFull, Bf[b], off, G);
+                    const double Bp = __shfl_up_sync(kFull, Bf[b], off);
                     if (lane >= off) Bf[b] += Af[k] * Bp;
                 }
             }
 #pragma unroll
             for (int b = 0; b < P; ++b) {
-                double d = __shfl_up_sync(kFull, Bf[b], 1, G);
+                double d = __shfl_up_sync(kFull, Bf[b], 1);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     const int i = i0 + e;
@@ -852,24 +842,24 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
                 Bb[b] = B;
             }
 #pragma unroll
-            for (int k = 0, off = 1; k < LG; ++k, off <<= 1) {
+            for (int k = 0, off = 1; k < 5; ++k, off <<= 1) {
 #pragma unroll
                 for (int b = 0; b < P; ++b) {
-                    const double Bp = __shfl_down_sync(kFull, Bb[b], off, G);
-                    if (lane + off < G) Bb[b] += Ab[k] * Bp;
+                    const double Bp = __shfl_down_sync(kFull, Bb[b], off);
+                    if (lane + off < 32) Bb[b] += Ab[k] * Bp;
                 }
             }
             const long long q0 = a.plane_of[l * (a.m0 + 1)] + j;
 #pragma unroll
             for (int b = 0; b < P; ++b) {
-                double x = __shfl_down_sync(kFull, Bb[b], 1, G);
+                double x = __shfl_down_sync(kFull, Bb[b], 1);
                 TP* g = planes + (q0 + b) * a.pstride + cell * n;
 #pragma unroll
                 for (int e = E - 1; e >= 0; --e) {
                     const int i = i0 + e;
                     if (i < n) {
                         x = (i == n - 1) ? cur[b][e] : cur[b][e] - cp[e] * x;
-                        if (valid && j + b < nq) g[i] = (TP)(x - ref_at(a, q0 + b, i));
+                        if (j + b < nq) g[i] = (TP)(x - ref_at(a, q0 + b, i));
                     }
                 }
             }
@@ -887,23 +877,6 @@ template <typename TP, int E, int P>
 __global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
     extern __shared__ double smem[];
     for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) collide_lane_cell<TP, E, P>(a, cell, smem);
-}
-
-// Two cells a warp (nump <= 128): each half-warp owns one cell and its own
-// work space (cell_doubles apart), so every per-cell scalar -- the Coulomb
-// logarithms, the low-v fit, the pivot recursion of each l -- serves two
-// cells per instruction, and the scans take four steps instead of five.
-// An odd last cell pairs with a copy of itself that stores nothing.
-template <typename TP, int E, int P>
-__global__ void __launch_bounds__(32) collide_lane2_kernel(const CollideArgs a, const int cell_doubles) {
-    extern __shared__ double smem[];
-    const int half = threadIdx.x >> 4;
-    for (long long c0 = 2 * (long long)blockIdx.x; c0 < a.cells; c0 += 2 * (long long)gridDim.x) {
-        const long long cell = c0 + half;
-        const bool valid = cell < a.cells;
-        collide_lane_cell<TP, E, P, 16>(a, valid ? cell : c0, smem + (size_t)half * cell_doubles, valid);
-        __syncwarp();
-    }
 }
 
 // batched form: work item = (problem, cell); the problems share E
@@ -993,35 +966,8 @@ cudaError_t launch_lane(const CollideArgs& a, cudaStream_t st, int blocks, size_
     collide_lane_kernel<TP, E, P><<<blocks, 32, smem, st>>>(a);
     return cudaGetLastError();
 }
-// two cells a warp: E = ceil(np/16) points a lane, the same register budget
-template <typename TP, int E>
-cudaError_t launch_lane2(const CollideArgs& a, cudaStream_t st, size_t smem_cell) {
-    constexpr int P = E <= 2 ? 4 : (E <= 4 ? 2 : 1);
-    const size_t smem = 2 * smem_cell;
-    {
-        const cudaError_t e = ensure_dyn_smem((const void*)collide_lane2_kernel<TP, E, P>, smem);
-        if (e != cudaSuccess) return e;
-    }
-    const long long pairs = (a.cells + 1) / 2;
-    const long long blocks = pairs < (1ll << 30) ? pairs : (1ll << 30);
-    collide_lane2_kernel<TP, E, P><<<(unsigned)blocks, 32, smem, st>>>(a, (int)(smem_cell / sizeof(double)));
-    return cudaGetLastError();
-}
 template <typename TP>
 cudaError_t launch_lane_e(const CollideArgs& a, cudaStream_t st, int blocks, size_t smem) {
-    if (a.np <= 128) {
-        switch ((a.np + 15) / 16) {
-            case 1: return launch_lane2<TP, 1>(a, st, smem);
-            case 2: return launch_lane2<TP, 2>(a, st, smem);
-            case 3: return launch_lane2<TP, 3>(a, st, smem);
-            case 4: return launch_lane2<TP, 4>(a, st, smem);
-            case 5: return launch_lane2<TP, 5>(a, st, smem);
-            case 6: return launch_lane2<TP, 6>(a, st, smem);
-            case 7: return launch_lane2<TP, 7>(a, st, smem);
-            case 8: return launch_lane2<TP, 8>(a, st, smem);
-            default: return cudaErrorInvalidValue;
-        }
-    }
     switch ((a.np + 31) / 32) {
         case 1: return launch_lane<TP, 1>(a, st, blocks, smem);
         case 2: return launch_lane<TP, 2>(a, st, blocks, smem);

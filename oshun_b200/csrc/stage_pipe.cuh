@@ -828,14 +828,18 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, (const TS*)nullptr, np);
+                    const TS* ref = a.pl_ref ? a.pl_ref + (long long)splane[s * mstride + m] * np : nullptr;
+                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, ref, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
+                            // the current of f = ref + stored deviation
+                            const double r0 = ref ? (double)ref[pc] : 0.0;
                             if constexpr (m == 0) {
-                                jx += wj * (double)sb[nb.ctr];
+                                jx += wj * ((double)sb[nb.ctr] + r0);
                             } else {
-                                jyr += wj * (double)sb[nb.ctr];
-                                jyi += wj * (double)sb[seg + nb.ctr];
+                                const double r1 = ref ? (double)ref[np + pc] : 0.0;
+                                jyr += wj * ((double)sb[nb.ctr] + r0);
+                                jyi += wj * ((double)sb[seg + nb.ctr] + r1);
                             }
                         }
                     }
