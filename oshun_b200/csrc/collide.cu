@@ -110,8 +110,11 @@ __device__ double zlog_ei(double ne, double Te, double density_np, double Zeta) 
 
 // The planes hold f - ref when a momentum profile is given (FP32 split):
 // f of plane q at momentum point p, and the stored value of f.
+// (FP64 planes hold f itself: no profile is read for them.)
+template <typename TP>
 __device__ __forceinline__ double ref_at(const CollideArgs& a, long long q, int p) {
-    return a.pl_ref ? a.pl_ref[q * a.np + p] : 0.0;
+    if constexpr (sizeof(TP) == sizeof(float)) return a.pl_ref ? a.pl_ref[q * a.np + p] : 0.0;
+    return 0.0;
 }
 
 struct Smem {
@@ -282,7 +285,7 @@ __device__ void tridiagonal_chunks(const CollideArgs& a, const Smem& s, long lon
         for (int idx = threadIdx.x; idx < nq * n; idx += blockDim.x) {
             const int j = idx / n, p = idx - j * n;
             s.chunk[(long long)j * 2 * ld + p] =
-                (double)planes[(long long)(q0 + j) * a.pstride + cell * n + p] + ref_at(a, q0 + j, p);
+                (double)planes[(long long)(q0 + j) * a.pstride + cell * n + p] + ref_at<TP>(a, q0 + j, p);
         }
         __syncthreads();
         for (int j = threadIdx.x; j < nq; j += blockDim.x) {
@@ -310,7 +313,7 @@ __device__ void tridiagonal_chunks(const CollideArgs& a, const Smem& s, long lon
             const int q = q0 + j;
             const int l = plane_l[q], m = plane_m[q];
             if (l < 1 || m > a.mmax_coll || (l == 1 ? !a.do_l1 : !a.do_lm)) continue;
-            planes[(long long)q * a.pstride + cell * n + p] = (TP)(s.chunk[(long long)j * 2 * ld + p] - ref_at(a, q, p));
+            planes[(long long)q * a.pstride + cell * n + p] = (TP)(s.chunk[(long long)j * 2 * ld + p] - ref_at<TP>(a, q, p));
         }
         __syncthreads();
     }
@@ -448,8 +451,8 @@ __device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell
                 const TP* pr_ = planes + q * a.pstride + cell * n;
                 const TP* pi_ = planes + (q + 1) * a.pstride + cell * n;
                 for (int k = threadIdx.x & 31; k < n; k += 32) {
-                    br[k] = (double)pr_[k] + ref_at(a, q, k);
-                    bi[k] = m > 0 ? (double)pi_[k] + ref_at(a, q + 1, k) : 0.0;
+                    br[k] = (double)pr_[k] + ref_at<TP>(a, q, k);
+                    bi[k] = m > 0 ? (double)pi_[k] + ref_at<TP>(a, q + 1, k) : 0.0;
                     xr[k] = br[k];
                     xi[k] = bi[k];
                 }
@@ -458,8 +461,8 @@ __device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell
                 TP* wr = planes + q * a.pstride + cell * n;
                 TP* wi = planes + (q + 1) * a.pstride + cell * n;
                 for (int k = threadIdx.x & 31; k < n; k += 32) {
-                    wr[k] = (TP)(xr[k] - ref_at(a, q, k));
-                    if (m > 0) wi[k] = (TP)(xi[k] - ref_at(a, q + 1, k));
+                    wr[k] = (TP)(xr[k] - ref_at<TP>(a, q, k));
+                    if (m > 0) wi[k] = (TP)(xi[k] - ref_at<TP>(a, q + 1, k));
                 }
                 __syncwarp();
             }
@@ -599,7 +602,7 @@ __global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
             const double* cpl = cp + (size_t)(l - 1) * n;
             const double* idl = idv + (size_t)(l - 1) * n;
             TP* g = planes + (long long)q * a.pstride + cell * n;
-            for (int k = lane; k < n; k += 32) row[k] = (double)g[k] + ref_at(a, q, k);
+            for (int k = lane; k < n; k += 32) row[k] = (double)g[k] + ref_at<TP>(a, q, k);
             __syncwarp();
             // forward: compose this lane's maps x -> A x + B over [rb, re)
             double A = 1.0, B = 0.0;
@@ -650,7 +653,7 @@ __global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
                 }
             }
             __syncwarp();
-            for (int k = lane; k < n; k += 32) g[k] = (TP)(row[k] - ref_at(a, q, k));
+            for (int k = lane; k < n; k += 32) g[k] = (TP)(row[k] - ref_at<TP>(a, q, k));
             __syncwarp();
         }
     }
@@ -720,7 +723,7 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
             const TP* g = planes + (q0 + b) * a.pstride + cell * n;
 #pragma unroll
             for (int e = 0; e < E; ++e)
-                r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] + ref_at(a, q0 + b, i0 + e) : 0.0;
+                r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] + ref_at<TP>(a, q0 + b, i0 + e) : 0.0;
         }
     };
 
@@ -859,7 +862,7 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
                     const int i = i0 + e;
                     if (i < n) {
                         x = (i == n - 1) ? cur[b][e] : cur[b][e] - cp[e] * x;
-                        if (j + b < nq) g[i] = (TP)(x - ref_at(a, q0 + b, i));
+                        if (j + b < nq) g[i] = (TP)(x - ref_at<TP>(a, q0 + b, i));
                     }
                 }
             }

@@ -8,6 +8,12 @@
 * The same two steps in the FP32/FP64 split form: the relative L2 error of
   every harmonic and field against the FP64 oracle, without a norm floor,
   held to the per-result bounds below (f_22 and B_z carry the 1e-6 seed).
+* A 128 x 8 strip of the same deck for 20 steps in the split form, every
+  harmonic and field held to its own bound (twice the value measured on a
+  B200): the m = 0 harmonics l = 1, 3, 4, 5, 6 carry small residuals of
+  large E-field and advection terms and grow to 1e-6 .. 2e-5 there (their
+  FP64 errors are 1e-11, against 1e-14 for the others, from the same
+  sensitivity); everything else stays below 5e-7.
 * 1D Landau damping, 64 cells, lmax = 8, np = 64, the full 1000 RK4 steps
   (dt = 0.05), FP64, <= 1e-12.
 
@@ -97,3 +103,20 @@ def test_landau_full_1000_steps(oracle):
     assert eE <= max(TOL, 2.0 * sE), (eE, sE)
     # the damped field is still resolved: E_x carries the wave after 1000 steps
     assert np.linalg.norm(ref.fields[0]) > 0
+
+
+# FP32/FP64 split, 128 x 8 strip, 20 steps: twice the measured relative L2
+# error of each result against the FP64 oracle (unfloored)
+STRIP_BOUNDS = {"f00": 1e-13, "f10": 2.5e-5, "f30": 4e-5, "f40": 8e-6, "f50": 3e-6, "f60": 1.3e-6,
+                "f20": 2e-9}
+STRIP_DEFAULT = 1e-6
+
+
+def test_weibel_strip_fp32_split_20_steps(oracle):
+    cfg, f, fields, _ = workloads.weibel2d(0, ny=8)
+    st = State(deck_of(cfg), f, fields)
+    ref = oracle.steps(st, 20, 15)
+    out = run_gpu(st, ["step:20:15"], fast_path=True, precision=1)
+    rows = per_result(out, ref)
+    bad = {k: v for k, v in rows.items() if not v <= STRIP_BOUNDS.get(k, STRIP_DEFAULT)}
+    assert not bad, bad
