@@ -50,6 +50,13 @@ typedef enum oshun_precision {
 #define OSHUN_FLAG_FIX_YADV_CHAIN 0x1  /* drop the reference's y-advection coefficient
                                           factor C1[l-1]/C1[m+1] that OSHUN-1 carries for
                                           m >= 2 (def-VlasovMax.cpp:916-946) */
+#define OSHUN_FLAG_IMPLICIT_EE 0x2     /* opt-in, not in the reference: the f00 e-e step
+                                          as one backward-Euler step over the whole
+                                          interval (three Picard sweeps of a per-cell
+                                          tridiagonal solve of the same discrete flux
+                                          operator) instead of the explicit RK4
+                                          substeps of Explicit_EC_FP::loop
+                                          (def-FokkerPlanck.cpp:590-625) */
 
 /* Run configuration: the input-deck fields the hot path reads
  * (OSHUN-1/decl-input.h:59-138, derived values as in

@@ -227,6 +227,7 @@ class Oracle:
         self.lib.oo_rhs.argtypes = [ctypes.POINTER(_OoDeck), dp, dp]
         self.lib.oo_steps.argtypes = [ctypes.POINTER(_OoDeck), dp, ctypes.c_int, ctypes.c_int]
         self.lib.oo_set_yadv_chain.argtypes = [ctypes.c_int]
+        self.lib.oo_set_ee_implicit.argtypes = [ctypes.c_int]
         self.lib.oo_nondominant_count.restype = ctypes.c_long
 
     @staticmethod
@@ -252,6 +253,11 @@ class Oracle:
 
     def set_yadv_chain(self, keep: bool) -> None:
         self.lib.oo_set_yadv_chain(1 if keep else 0)
+
+    def set_ee_implicit(self, sweeps: int) -> None:
+        """0: the reference's explicit e-e substeps; > 0: the opt-in
+        backward-Euler e-e step with that many Picard sweeps."""
+        self.lib.oo_set_ee_implicit(int(sweeps))
 
     def nondominant(self) -> int:
         return int(self.lib.oo_nondominant_count())

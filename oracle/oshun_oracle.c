@@ -557,6 +557,115 @@ static void collide_ee(const Grid* g, const VGrid* v, cplx* Y, double hstep, int
     free(buf);
 }
 
+/* Opt-in backward-Euler e-e step (not a reference scheme; the checker of
+ * OSHUN_FLAG_IMPLICIT_EE).  The explicit operator of ee_slope is
+ *   C(f)_k = c_kpre lnee Qn_k (D_{k-1} - D_k),  D_k = P_k (G_k - G_{k+1}),
+ *   G_j = A_j f_j - B_j  (A = I4 + v^3 J1, B = 3 I2 J1; the low-v fit's
+ *   i4s, i2s for j < NB), row 0: Qn_0 (-(2/v_0^2) G_0 - D_0), D_{n-1} = G_{n-1}.
+ * One step g - D C(g) = f over the whole interval D is solved by Picard
+ * sweeps, each a tridiagonal solve with the coefficients from the previous
+ * iterate x (the first from f): on each face the B difference becomes a drag
+ * on g, B_{k+1} - B_k = gam_k ((1 - w) g_k + w g_{k+1}) with
+ * gam_k = (B_{k+1} - B_k) / ((1 - w) x_k + w x_{k+1}), w = 1/2, or 0 / 1
+ * (upwind) where 1/2 would give the face a coefficient of the wrong sign;
+ * likewise B_0 = (B_0 / x_0) g_0.  So every sweep's matrix is an M-matrix
+ * (the step keeps f positive for any D) and at convergence (g = x) the
+ * operator is the explicit one exactly: the step converges to the explicit
+ * scheme as D -> 0 and moves number and energy as it does. */
+static int g_ee_sweeps = 0;
+void oo_set_ee_implicit(int sweeps) { g_ee_sweeps = sweeps > 0 ? sweeps : 0; }
+
+/* face k (between points k and k+1): D_k = al g_k + be g_{k+1} + cs; the
+ * B difference stays explicit (cs) where the iterate is not positive there */
+static void ee_face(double Ak, double Ak1, double Bk, double Bk1, double xk, double xk1, double P,
+                    double* al, double* be, double* cs) {
+    const double dB = Bk1 - Bk;
+    const double h = 0.5 * (xk + xk1);
+    *cs = 0.0;
+    if (!(h > 0.0)) {
+        *al = P * Ak; *be = -P * Ak1; *cs = P * dB;
+        return;
+    }
+    double w = 0.5;
+    double gam = dB / h;
+    if (Ak + 0.5 * gam < 0.0) w = 1.0;          /* gam < 0: all of it on g_{k+1} */
+    else if (0.5 * gam > Ak1) w = 0.0;          /* gam > 0: all of it on g_k */
+    if (w != 0.5) {
+        const double hw = (1.0 - w) * xk + w * xk1;
+        if (!(hw > 0.0)) { *al = P * Ak; *be = -P * Ak1; *cs = P * dB; return; }
+        gam = dB / hw;
+    }
+    *al = P * (Ak + gam * (1.0 - w));
+    *be = P * (gam * w - Ak1);
+}
+
+static void collide_ee_be(const Grid* g, const VGrid* v, cplx* Y, double D, int sweeps) {
+    const int n = g->np;
+    const double* vr = v->vr;
+    const double v0s = vr[0] * vr[0], v1s = vr[1] * vr[1];
+    double kp = sqrt(4.0 * M_PI * g->d->density_np * RE_CLASSICAL);
+    const double c_kpre = 4.0 * M_PI / 3.0 * RE_CLASSICAL * kp;
+    double* buf = (double*)calloc((size_t)13 * n, sizeof(double));
+    double *I4 = buf, *I2 = buf + n, *J1 = buf + 2 * n, *f = buf + 3 * n, *x = buf + 4 * n;
+    double *A = buf + 5 * n, *B = buf + 6 * n, *al = buf + 7 * n, *be = buf + 8 * n;
+    double *tb = buf + 9 * n, *r = buf + 10 * n, *cp = buf + 11 * n, *cs = buf + 12 * n;
+    cplx* f00 = Y + IND(g, 0, 0) * g->hsize;
+    for (long c = 0; c < g->cells; ++c) {
+        for (int p = 0; p < n; ++p) { f[p] = creal(f00[c * n + p]); x[p] = f[p]; }
+        for (int sw = 0; sw < sweeps; ++sw) {
+            I4[0] = 0; I2[0] = 0; J1[n - 1] = 0;
+            for (int k = 1; k < n; ++k) I4[k] = I4[k - 1] + (v->U4[k] * x[k] + v->U4m1[k] * x[k - 1]);
+            for (int k = 1; k < n; ++k) I2[k] = I2[k - 1] + (v->U2[k] * x[k] + v->U2m1[k] * x[k - 1]);
+            for (int k = n - 2; k >= 0; --k) J1[k] = J1[k + 1] + (v->U1[k + 1] * x[k + 1] + v->U1m1[k + 1] * x[k]);
+            const double lnee = log_ee(g->d, 4.0 * M_PI * I2[n - 1], 4.0 * M_PI * I4[n - 1]);
+            const double dn = D * c_kpre * lnee;
+            const double fz = (x[0] - x[1] * v0s / v1s) / (1.0 - v0s / v1s);
+            for (int k = 0; k < n; ++k) {
+                double i4 = I4[k], i2 = I2[k];
+                const double v3 = pow(vr[k], 3);
+                if (k < g->d->NB_algorithms) {
+                    i2 = fz * v3 / 3.0 + (x[1] - fz) * pow(vr[k], 5) / v1s * 0.2;
+                    i4 = fz * pow(vr[k], 5) * 0.2 + (x[1] - fz) * pow(vr[k], 7) / (v1s * 7.0);
+                }
+                A[k] = i4 + v3 * J1[k];
+                B[k] = 3.0 * i2 * J1[k];
+            }
+            for (int k = 0; k < n - 1; ++k)
+                ee_face(A[k], A[k + 1], B[k], B[k + 1], x[k], x[k + 1], v->Pn[k], al + k, be + k, cs + k);
+            /* rows of M = I - dn W': sub -dn Qn al_{k-1}, diagonal, super dn Qn be_k
+             * (as in Thomas below); the explicit parts go to the right-hand side */
+            const int imp0 = x[0] > 0.0;
+            const double a0 = imp0 ? A[0] - B[0] / x[0] : A[0];
+            const double b0 = imp0 ? 0.0 : B[0];
+            for (int k = 0; k < n; ++k) {
+                const double q = v->Qn[k];
+                double d0, c0;
+                if (k == 0) { d0 = -q * ((2.0 / v0s) * a0 + al[0]); c0 = q * ((2.0 / v0s) * b0 - cs[0]); }
+                else if (k < n - 1) { d0 = q * (be[k - 1] - al[k]); c0 = q * (cs[k - 1] - cs[k]); }
+                else { d0 = q * (be[k - 1] - A[k]); c0 = q * cs[k - 1]; }
+                tb[k] = 1.0 - dn * d0;
+                r[k] = f[k] + dn * c0;
+            }
+            /* Thomas: sub_k = -dn Qn_k al_{k-1}, super_k = dn Qn_k be_k */
+            {
+                double sup = dn * v->Qn[0] * be[0];
+                cp[0] = sup / tb[0];
+                x[0] = r[0] / tb[0];
+                for (int k = 1; k < n; ++k) {
+                    const double sub = -dn * v->Qn[k] * al[k - 1];
+                    sup = k < n - 1 ? dn * v->Qn[k] * be[k] : 0.0;
+                    const double id = 1.0 / (tb[k] - sub * cp[k - 1]);
+                    cp[k] = sup * id;
+                    x[k] = (r[k] - sub * x[k - 1]) * id;
+                }
+                for (int k = n - 2; k >= 0; --k) x[k] -= cp[k] * x[k + 1];
+            }
+        }
+        for (int p = 0; p < n; ++p) f00[c * n + p] = x[p];
+    }
+    free(buf);
+}
+
 /* ------------------------------------------------------------------------ */
 /* implicit f_lm: Implicit_FLM_step (def-FokkerPlanck.cpp:757-1035)          */
 /* ------------------------------------------------------------------------ */
@@ -792,7 +901,8 @@ int oo_steps(const oo_deck* d, double* state, int nsteps, int mask) {
         if (mask & 2) {
             int nsub = (int)((t - t_ee) / d->small_dt) + 1;
             double hh = (t - t_ee) / (double)nsub;
-            collide_ee(&g, &v, Y, hh, nsub);
+            if (g_ee_sweeps > 0) collide_ee_be(&g, &v, Y, t - t_ee, g_ee_sweeps);
+            else collide_ee(&g, &v, Y, hh, nsub);
             t_ee = t;
         }
         if (mask & 12) collide_flm(&g, &v, Y, t - t_eb, (mask & 4) != 0, (mask & 8) != 0);

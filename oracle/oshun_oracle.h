@@ -30,6 +30,11 @@ typedef struct oo_deck {
  * chain factor for m >= 2 (see oo_yadv_factor in oshun_oracle.c) */
 void oo_set_yadv_chain(int keep);
 
+/* e-e step of later oo_steps calls: 0 (default) the reference's explicit RK4
+ * substeps; sweeps > 0 the opt-in backward-Euler step with that many Picard
+ * sweeps (OSHUN_FLAG_IMPLICIT_EE of the CUDA path) */
+void oo_set_ee_implicit(int sweeps);
+
 long oo_state_doubles(const oo_deck* d);
 
 /* slope = Actions::Adv(state) */

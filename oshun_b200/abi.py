@@ -18,6 +18,7 @@ LIB_PATH = os.environ.get("OSHUN_B200_LIB") or os.path.join(HERE, "liboshun_b200
 OSHUN_FP64 = 0
 OSHUN_FP32_SPLIT = 1
 OSHUN_FLAG_FIX_YADV_CHAIN = 0x1
+OSHUN_FLAG_IMPLICIT_EE = 0x2      # opt-in backward-Euler f00 e-e step (not a reference scheme)
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_UNSUPPORTED", 3: "ERR_CUDA", 4: "ERR_NONREAL",
           5: "ERR_NUMERIC", 6: "ERR_NO_DEVICE"}

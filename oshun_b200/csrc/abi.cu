@@ -625,6 +625,7 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     a.do_ee = do_ee; a.do_l1 = do_l1; a.do_lm = do_lm;
     a.if_tridiagonal = c.if_tridiagonal;
     a.nsub = nsub; a.hsub = hsub; a.Dt = Dt;
+    a.ee_implicit = (c.flags & OSHUN_FLAG_IMPLICIT_EE) ? kEeImplicitSweeps : 0;
     a.NB = c.NB_algorithms;
     a.density_np = c.density_np; a.Zeta = c.Zeta;
     a.c_kpre = h->c_kpre; a.kpre = h->kpre;
@@ -638,8 +639,16 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     return a;
 }
 
-int launch_collide_args(oshun_ctx* h, const CollideArgs& a) {
+int launch_collide_args(oshun_ctx* h, const CollideArgs& a0) {
     cudaError_t e;
+    CollideArgs a = a0;
+    if (a.do_ee && a.ee_implicit > 0) {
+        // the backward-Euler e-e step in its own launch, then the f_lm solves
+        e = launch_ee_implicit(a, h->stream);
+        if (e != cudaSuccess) { set_error(std::string("e-e launch: ") + cudaGetErrorString(e)); return OSHUN_ERR_CUDA; }
+        a.do_ee = 0;
+        if (!a.do_l1 && !a.do_lm) return OSHUN_OK;
+    }
     if (h->tri_cpc > 0)
         e = launch_collide_tri(a, h->stream, h->tri_cpc, h->tri_blocks);
     else
@@ -1621,6 +1630,10 @@ int oshun_batch_create(const oshun_cfg* cfgs, int n, const int* collide, oshun_b
         }
         const int col = collide ? (collide[i] != 0) : 1;
         if (col && !c.if_tridiagonal) { set_error("batched collision steps are tridiagonal"); return fail(OSHUN_ERR_UNSUPPORTED); }
+        if (col && (c.flags & OSHUN_FLAG_IMPLICIT_EE)) {
+            set_error("batched collision steps use the explicit e-e substeps");
+            return fail(OSHUN_ERR_UNSUPPORTED);
+        }
         oshun_handle h = nullptr;
         int rc = oshun_create(&c, &h);
         if (rc) return fail(rc);
@@ -2079,6 +2092,10 @@ int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out) {
     if (cfg->numy != 1 || cfg->m0 != 0 || cfg->precision != OSHUN_FP64 || !cfg->if_tridiagonal ||
         ((cfg->nump + 31) / 32) * 32 > 256) {
         set_error("the adjoint covers 1D runs (numy = 1) with m0 = 0, FP64, tridiagonal collisions, nump <= 256");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
+    if (cfg->flags & OSHUN_FLAG_IMPLICIT_EE) {
+        set_error("the adjoint transposes the explicit e-e substeps, not the implicit e-e step");
         return OSHUN_ERR_UNSUPPORTED;
     }
     oshun_adj_ctx* a = new oshun_adj_ctx();

@@ -474,6 +474,115 @@ __device__ void dense_solves(const CollideArgs& a, const Smem& s, long long cell
     }
 }
 
+// Opt-in backward-Euler e-e step (OSHUN_FLAG_IMPLICIT_EE; not a reference
+// scheme) on one warp, f00 of the cell in s.f.  The explicit operator of
+// EE_isotropic_conserva (def-FokkerPlanck.cpp:201-267) is
+//   C(f)_k = c_kpre lnee Qn_k (D_{k-1} - D_k),  D_k = P_k (G_k - G_{k+1}),
+//   G_j = A_j f_j - B_j  (A = I4 + v^3 J1, B = 3 I2 J1; the low-v fit's
+//   i4s, i2s for j < NB); row 0 Qn_0 (-(2/v_0^2) G_0 - D_0), D_{n-1} = G_{n-1}.
+// One step g - D C(g) = f over the whole e-e interval D, by Picard sweeps,
+// each a tridiagonal solve with the coefficients of the previous iterate x
+// (the first from f): on each face the B difference becomes a drag on g,
+// B_{k+1} - B_k = gam_k ((1 - w) g_k + w g_{k+1}), gam_k = (B_{k+1} - B_k) /
+// ((1 - w) x_k + w x_{k+1}), w = 1/2, or 0 / 1 (upwind) where 1/2 would give
+// the face a coefficient of the wrong sign; likewise B_0 = (B_0 / x_0) g_0.
+// Every sweep's matrix is then an M-matrix (f stays positive for any D),
+// and at convergence (g = x) the operator is the explicit one exactly, so
+// the step converges to the explicit scheme as D -> 0.
+// face k (between points k and k+1): D_k = al g_k + be g_{k+1} + cs; the
+// B difference stays explicit (cs) where the iterate is not positive there
+__device__ __forceinline__ void ee_face(double Ak, double Ak1, double Bk, double Bk1, double xk, double xk1,
+                                        double P, double& al, double& be, double& cs) {
+    const double dB = Bk1 - Bk;
+    const double h = 0.5 * (xk + xk1);
+    cs = 0.0;
+    if (!(h > 0.0)) { al = P * Ak; be = -P * Ak1; cs = P * dB; return; }
+    double w = 0.5;
+    double gam = dB / h;
+    if (Ak + 0.5 * gam < 0.0) w = 1.0;
+    else if (0.5 * gam > Ak1) w = 0.0;
+    if (w != 0.5) {
+        const double hw = (1.0 - w) * xk + w * xk1;
+        if (!(hw > 0.0)) { al = P * Ak; be = -P * Ak1; cs = P * dB; return; }
+        gam = dB / hw;
+    }
+    al = P * (Ak + gam * (1.0 - w));
+    be = P * (gam * w - Ak1);
+}
+__device__ void ee_implicit_step(const CollideArgs& a, const Smem& s) {
+    const StepP sp = step_params(a);
+    const double D = a.clock ? (a.clock[0] - a.clock[1]) : sp.hsub * (double)sp.nsub;
+    const int n = a.np;
+    const int lane = threadIdx.x & 31;
+    const double* vr = a.vr;
+    const double v0s = vr[0] * vr[0], v1s = vr[1] * vr[1];
+    double* x = s.f1;    // iterate
+    double* A = s.f0;    // A_j, then the Thomas c'
+    double* B = s.fh;    // B_j
+    double* al = s.tri_a;
+    double* be = s.tri_c;
+    double* tb = s.tri_b;
+    double* cs = s.scat;   // explicit face parts
+    for (int k = lane; k < n; k += 32) x[k] = s.f[k];
+    __syncwarp();
+    for (int sweep = 0; sweep < a.ee_implicit; ++sweep) {
+        warp_cumsum3(s.I4, s.I2, s.J1, n, [&](int k) { return a.U4[k] * x[k] + a.U4m1[k] * x[k - 1]; },
+                     [&](int k) { return a.U2[k] * x[k] + a.U2m1[k] * x[k - 1]; },
+                     [&](int i) { return a.U1[i] * x[i] + a.U1m1[i] * x[i - 1]; });
+        const double lnee = log_ee(4.0 * M_PI * s.I2[n - 1], 4.0 * M_PI * s.I4[n - 1], a.density_np);
+        const double dn = D * a.c_kpre * lnee;
+        const double fz = (x[0] - x[1] * v0s / v1s) / (1.0 - v0s / v1s);
+        for (int k = lane; k < n; k += 32) {
+            const double j1 = s.J1[k], v3 = a.U3[k];
+            double i4 = s.I4[k], i2 = s.I2[k];
+            if (k < a.NB) {
+                i2 = fz * v3 / 3.0 + (x[1] - fz) * a.V5[k] / v1s * 0.2;
+                i4 = fz * a.V5[k] * 0.2 + (x[1] - fz) * a.V7[k] / (v1s * 7.0);
+            }
+            A[k] = i4 + v3 * j1;
+            B[k] = 3.0 * i2 * j1;
+        }
+        __syncwarp();
+        for (int k = lane; k < n - 1; k += 32)
+            ee_face(A[k], A[k + 1], B[k], B[k + 1], x[k], x[k + 1], a.Pn[k], al[k], be[k], cs[k]);
+        __syncwarp();
+        const bool imp0 = x[0] > 0.0;
+        const double a0 = imp0 ? A[0] - B[0] / x[0] : A[0];
+        const double b0 = imp0 ? 0.0 : B[0];
+        double* rhs = s.I2;   // free once A and B are formed
+        for (int k = lane; k < n; k += 32) {
+            const double q = a.Qn[k];
+            double d0, c0;
+            if (k == 0) { d0 = -q * ((2.0 / v0s) * a0 + al[0]); c0 = q * ((2.0 / v0s) * b0 - cs[0]); }
+            else if (k < n - 1) { d0 = q * (be[k - 1] - al[k]); c0 = q * (cs[k - 1] - cs[k]); }
+            else { d0 = q * (be[k - 1] - A[k]); c0 = q * cs[k - 1]; }
+            tb[k] = 1.0 - dn * d0;
+            rhs[k] = s.f[k] + dn * c0;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            // Thomas: sub-diagonal -dn Qn_k al_{k-1}, super-diagonal dn Qn_k be_k;
+            // c' into A, d' then the solution into x
+            double sup = dn * a.Qn[0] * be[0];
+            double cp = sup / tb[0];
+            double dp = rhs[0] / tb[0];
+            A[0] = cp; x[0] = dp;
+            for (int k = 1; k < n; ++k) {
+                const double sub = -dn * a.Qn[k] * al[k - 1];
+                sup = k < n - 1 ? dn * a.Qn[k] * be[k] : 0.0;
+                const double id = 1.0 / (tb[k] - sub * cp);
+                cp = sup * id;
+                dp = (rhs[k] - sub * dp) * id;
+                A[k] = cp; x[k] = dp;
+            }
+            for (int k = n - 2; k >= 0; --k) x[k] -= A[k] * x[k + 1];
+        }
+        __syncwarp();
+    }
+    for (int k = lane; k < n; k += 32) s.f[k] = x[k];
+    __syncwarp();
+}
+
 // e-e RK4 substeps of Explicit_EC_FP::loop on one warp (f00 of the cell in s.f)
 __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
     const StepP sp = step_params(a);
@@ -504,6 +613,22 @@ __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
         __syncwarp();
         ee_slope(a, s, s.f0, s.fh);
         for (int k = lane; k < n; k += 32) s.f[k] += s.fh[k] * (h / 6.0);
+        __syncwarp();
+    }
+}
+
+// the backward-Euler e-e step alone, one warp per cell (the collision
+// kernels then run with do_ee = 0)
+__global__ void __launch_bounds__(32) ee_implicit_kernel(const CollideArgs a) {
+    extern __shared__ double smem[];
+    const int n = a.np;
+    const Smem s = carve(smem, n);
+    const int lane = threadIdx.x & 31;
+    for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) {
+        for (int k = lane; k < n; k += 32) s.f[k] = a.f00[cell * n + k];
+        __syncwarp();
+        ee_implicit_step(a, s);
+        for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
         __syncwarp();
     }
 }
@@ -925,6 +1050,17 @@ __global__ void __launch_bounds__(256, 1) collide_lane_chunk_kernel(const Collid
 }
 
 }  // namespace
+
+cudaError_t launch_ee_implicit(const CollideArgs& a, cudaStream_t st) {
+    const size_t smem = ((size_t)kSmemArrays * a.np + kSmemScalars) * sizeof(double);
+    {
+        const cudaError_t e = ensure_dyn_smem((const void*)ee_implicit_kernel, smem);
+        if (e != cudaSuccess) return e;
+    }
+    const long long blocks = a.cells < (1ll << 30) ? a.cells : (1ll << 30);
+    ee_implicit_kernel<<<(unsigned)blocks, 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
 
 size_t collide_smem_bytes(int np, int chunk, int if_tridiagonal) {
     size_t base = ((size_t)kSmemArrays * np + kSmemScalars) * sizeof(double);

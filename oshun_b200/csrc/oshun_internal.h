@@ -17,6 +17,8 @@ namespace oshun {
 constexpr int kMaxM0 = 8;
 // Largest nump (threads of one cell row are one CTA dimension).
 constexpr int kMaxNp = 1024;
+// Picard sweeps of the opt-in backward-Euler e-e step (OSHUN_FLAG_IMPLICIT_EE)
+constexpr int kEeImplicitSweeps = 3;
 
 // Coupling coefficients of one source harmonic (l,m).  Each names the target
 // it feeds; a coefficient of a target that does not exist is 0 and the
@@ -101,6 +103,7 @@ struct CollideArgs {
     int do_ee, do_l1, do_lm;
     int if_tridiagonal;
     int nsub;             // e-e RK4 substeps
+    int ee_implicit;      // > 0: the e-e step is the backward-Euler one (launch_ee_implicit), this many sweeps
     double hsub;          // e-e substep
     double Dt;            // implicit step
     int NB;
@@ -116,6 +119,9 @@ struct CollideArgs {
     const double* clock;
     double small_dt;
 };
+
+// opt-in backward-Euler e-e step (a.ee_implicit sweeps), one warp per cell
+cudaError_t launch_ee_implicit(const CollideArgs& a, cudaStream_t st);
 
 // batched collision launch: CollideArgs per problem, (problem, cell) work items
 struct CollideBatch {

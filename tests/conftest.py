@@ -22,3 +22,4 @@ def oracle():
     orc = Oracle()
     yield orc
     orc.set_yadv_chain(True)
+    orc.set_ee_implicit(0)
