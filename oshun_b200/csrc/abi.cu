@@ -616,6 +616,7 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     a.f00 = h->f00[set];
     a.planes = h->pl[set];
     a.pl_ref = h->use_profile ? h->d_ref64 : nullptr;
+    a.pl_ref32 = h->use_profile ? (const float*)h->d_ref_ts : nullptr;
     a.planes_fp32 = h->fp32 ? 1 : 0;
     a.plane_of = h->d_plane_of; a.plane_l = h->d_plane_l; a.plane_m = h->d_plane_m;
     a.nplanes = h->nplanes;

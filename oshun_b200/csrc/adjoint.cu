@@ -5,18 +5,19 @@
 //                      of every f_l(x, p) (transposed G/H stencils, x
 //                      advection, current) and its share of the E_x(x)
 //                      cotangent, summed over the CTA in a fixed order;
-//   collide_adj_kernel the collision step's transpose, one thread per cell
-//                      (reverse sweep through the e-e RK4 substeps, the
-//                      transposed Thomas solves and the dependence of the
-//                      tridiagonal coefficients on f00), one cell a CTA with
-//                      its work space in shared memory where it fits (the
-//                      sweep is a long serial chain of work-space accesses:
-//                      shared memory instead of L2 shortens every link), else
-//                      in global memory;
+//   collide_adj_kernel the collision step's transpose (reverse sweep through
+//                      the e-e RK4 substeps, the transposed Thomas solves and
+//                      the dependence of the tridiagonal coefficients on f00),
+//                      one warp per cell (adjoint_warp.cuh: lane-parallel
+//                      maps, warp scans for the cumulative integrals and
+//                      their transposes, Thomas on lane 0), the cell's work
+//                      space in shared memory where it fits, else in global
+//                      memory;
 //   rk_combine_kernel  the linear combinations of the RK4 transpose.
 // State vectors use the plane layout: f00 plane, the l >= 1 planes, the 6
 // field planes (for m0 = 0 and numy = 1: f[l][x][p] then E_x[x], ...).
 #include "adjoint_math.h"
+#include "adjoint_warp.cuh"
 #include "oshun_internal.h"
 
 namespace oshun {
@@ -52,18 +53,17 @@ __global__ void stage_vjp_kernel(const Grid1 g, const double* __restrict__ s, co
     }
 }
 
-__global__ void collide_adj_kernel(const CollTables T, const int l0, const int nx, const double* __restrict__ y,
-                                   double* __restrict__ lam, const int ee, const int eb, const int nsub,
-                                   const double hsub, const double Dt, double* __restrict__ ws, const long long wsz,
-                                   const int smem_ws) {
+__global__ void __launch_bounds__(32) collide_adj_kernel(const CollTables T, const int l0, const double* __restrict__ y,
+                                                         double* __restrict__ lam, const int ee, const int eb,
+                                                         const int nsub, const double hsub, const double Dt,
+                                                         double* __restrict__ ws, const long long wsz,
+                                                         const int smem_ws, const long long pstride) {
     extern __shared__ double sws[];
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= nx) return;
+    const long long x = blockIdx.x;
     const int np = T.np;
-    const long long pstride = (long long)nx * np;
-    double* w = smem_ws ? sws : ws + x * wsz;   // smem_ws: one thread a CTA
-    adj::collide_cell_T(T, l0, y + (long long)x * np, y + pstride + (long long)x * np, pstride, ee, eb, nsub, hsub,
-                        Dt, lam + (long long)x * np, lam + pstride + (long long)x * np, pstride, w);
+    double* w = smem_ws ? sws : ws + x * wsz;
+    adjw::collide_cell_T(T, l0, y + x * np, y + pstride + x * np, pstride, ee, eb, nsub, hsub, Dt, lam + x * np,
+                         lam + pstride + x * np, pstride, w);
 }
 
 // out = a0 * v0 + a1 * v1 (+ a2 * v2)
@@ -87,13 +87,17 @@ cudaError_t launch_stage_vjp(const Grid1& g, const double* s, const double* c, d
 
 cudaError_t launch_collide_adj(const CollTables& T, int l0, int nx, const double* y, double* lam, int ee, int eb,
                                int nsub, double hsub, double Dt, double* ws, long long wsz, cudaStream_t st) {
-    const size_t smem = sizeof(double) * (size_t)wsz;
+    // wsz: the serial form's work space per cell (adj::coll_ws), at least the warp form's
+    const long long need = adjw::coll_ws(T.np, nsub);
+    if (need > wsz) return cudaErrorInvalidValue;
+    const long long pstride = (long long)nx * T.np;
+    const size_t smem = sizeof(double) * (size_t)need;
     if (smem <= 200 * 1024) {
         const cudaError_t e = ensure_dyn_smem((const void*)collide_adj_kernel, smem);
         if (e != cudaSuccess) return e;
-        collide_adj_kernel<<<nx, 1, smem, st>>>(T, l0, nx, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz, 1);
+        collide_adj_kernel<<<nx, 32, smem, st>>>(T, l0, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz, 1, pstride);
     } else {
-        collide_adj_kernel<<<(nx + 63) / 64, 64, 0, st>>>(T, l0, nx, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz, 0);
+        collide_adj_kernel<<<nx, 32, 0, st>>>(T, l0, y, lam, ee, eb, nsub, hsub, Dt, ws, wsz, 0, pstride);
     }
     return cudaGetLastError();
 }

@@ -94,6 +94,7 @@ struct CollideArgs {
     void* planes;         // l >= 1 planes (double or float)
     int planes_fp32;
     const double* pl_ref; // [nplanes][np] momentum profile the planes are stored relative to (null: none)
+    const float* pl_ref32;   // the same profile in FP32 (it is FP32-rounded: the values are equal)
     const int* plane_of;  // [(l0+1)*(m0+1)]
     const int* plane_l;   // [nplanes]: l of each plane
     const int* plane_m;   // [nplanes]: m of each plane
