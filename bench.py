@@ -464,37 +464,47 @@ def form_adjoint(stream, nsteps: int = 500, every: int = 50, cell: int = 256) ->
     """The sensitivity configuration (1D, nx = 512, lmax = 2, np = 128): one
     gradient of the time-integrated heat flux of one cell with respect to
     every cell's initial temperature, forward and checkpointed backward
-    through the adjoint kernels (FP64), timed with CUDA events."""
+    through the adjoint kernels, timed with CUDA events; FP64 and the FP32
+    bulk form (its gradient's largest deviation from the FP64 one, relative
+    to the largest FP64 component)."""
     import torch
     from oshun_b200 import workloads
     from oshun_b200.adjoint import Run, StepsWithCheckpoints, heat_flux_weight
     cfg, tau, _ = workloads.sensitivity1d()
-    run = Run(**cfg)
     w = heat_flux_weight(cfg, cell)
 
-    def grad_once():
-        t = torch.tensor(tau, device="cuda").requires_grad_(True)
-        y0 = workloads.sensitivity_state(cfg, t)
-        Q = StepsWithCheckpoints.apply(y0, run, nsteps, every, w)
-        Q.backward()
-        return t.grad
+    def timed(prec):
+        run = Run(**dict(cfg, precision=prec))
 
-    with torch.cuda.stream(stream):
-        grad_once()                      # warm-up
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        g = grad_once()
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    run.close()
+        def grad_once():
+            t = torch.tensor(tau, device="cuda").requires_grad_(True)
+            y0 = workloads.sensitivity_state(cfg, t)
+            Q = StepsWithCheckpoints.apply(y0, run, nsteps, every, w)
+            Q.backward()
+            return t.grad
+
+        with torch.cuda.stream(stream):
+            grad_once()                      # warm-up
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            g = grad_once()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        run.close()
+        return e0.elapsed_time(e1), g.detach().cpu().numpy()
+
+    ms, g = timed(0)
+    ms32, g32 = timed(1)
     coefs = (cfg["l0"] + 1) * cfg["numx"] * cfg["nump"]
+    scale = float(np.max(np.abs(g)))
     return {"workload": "sensitivity1d (nx=512, lmax=2, np=128)", "precision": "fp64", "steps": nsteps,
             "checkpoint_every": every, "ms_per_gradient": ms,
             "forward_steps_per_gradient": 2 * nsteps - nsteps // every, "vjp_steps_per_gradient": nsteps,
             "value": coefs * nsteps / (ms * 1e-3), "unit": UNIT + " (forward steps of the gradient's trajectory)",
-            "grad_finite": bool(torch.isfinite(g).all().item())}
+            "grad_finite": bool(np.isfinite(g).all()),
+            "fp32_bulk": {"ms_per_gradient": ms32, "value": coefs * nsteps / (ms32 * 1e-3),
+                          "max_dev_vs_fp64_grad": float(np.max(np.abs(g32 - g))) / scale if scale > 0 else None}}
 
 
 def run_ours(args, ws, rank, local):

@@ -268,7 +268,11 @@ int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile
 /* ---- adjoint of the small step ------------------------------------------- */
 
 /* No counterpart in the reference, which computes no derivatives.  For 1D
- * runs with m0 = 0 (numy = 1, FP64, tridiagonal collisions, nump <= 256):
+ * runs with m0 = 0 (numy = 1, tridiagonal collisions, nump <= 256), FP64 or
+ * the FP32 bulk form (precision OSHUN_FP32_SPLIT: the forward steps keep the
+ * l >= 1 planes and fields in FP32, and the stage transposes run in FP32
+ * arithmetic; f00, the collision transposes and the cotangent vectors stay
+ * FP64; the flag OSHUN_FLAG_IMPLICIT_EE is refused):
  * the vector-Jacobian product of one small step (oshun_step's sequence:
  * RK4 Vlasov-Maxwell step, then, with `collisions`, the e-e substeps and the
  * implicit f_l solves).  State vectors are device arrays of

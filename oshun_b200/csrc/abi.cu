@@ -2036,20 +2036,34 @@ struct oshun_adj_ctx {
 
 namespace {
 
+// FP64 state vector <-> handle set; an FP32-split handle rounds the planes
+// and fields to FP32 on the way in (f00 stays FP64)
 int adj_copy_in(oshun_ctx* h, int set, const double* y) {
     const size_t pb = sizeof(double) * h->pstride;
+    const long long npl = (long long)h->nplanes * h->pstride;
+    const double* yf = y + (1 + (long long)h->nplanes) * h->pstride;
     CK(cudaMemcpyAsync(h->f00[set], y, pb, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->pl[set], y + h->pstride, pb * h->nplanes, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->fld[set], y + (1 + (long long)h->nplanes) * h->pstride, sizeof(double) * 6 * h->cells,
-                       cudaMemcpyDeviceToDevice, h->stream));
+    if (h->fp32) {
+        CK(launch_convert(y + h->pstride, (float*)h->pl[set], npl, h->stream));
+        CK(launch_convert(yf, (float*)h->fld[set], 6 * h->cells, h->stream));
+    } else {
+        CK(cudaMemcpyAsync(h->pl[set], y + h->pstride, pb * h->nplanes, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->fld[set], yf, sizeof(double) * 6 * h->cells, cudaMemcpyDeviceToDevice, h->stream));
+    }
     return OSHUN_OK;
 }
 int adj_copy_out(oshun_ctx* h, int set, double* y) {
     const size_t pb = sizeof(double) * h->pstride;
+    const long long npl = (long long)h->nplanes * h->pstride;
+    double* yf = y + (1 + (long long)h->nplanes) * h->pstride;
     CK(cudaMemcpyAsync(y, h->f00[set], pb, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(y + h->pstride, h->pl[set], pb * h->nplanes, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(y + (1 + (long long)h->nplanes) * h->pstride, h->fld[set], sizeof(double) * 6 * h->cells,
-                       cudaMemcpyDeviceToDevice, h->stream));
+    if (h->fp32) {
+        CK(launch_convert((const float*)h->pl[set], y + h->pstride, npl, h->stream));
+        CK(launch_convert((const float*)h->fld[set], yf, 6 * h->cells, h->stream));
+    } else {
+        CK(cudaMemcpyAsync(y + h->pstride, h->pl[set], pb * h->nplanes, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(yf, h->fld[set], sizeof(double) * 6 * h->cells, cudaMemcpyDeviceToDevice, h->stream));
+    }
     return OSHUN_OK;
 }
 
@@ -2090,9 +2104,8 @@ extern "C" {
 int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out) {
     if (!out || !cfg) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
     *out = nullptr;
-    if (cfg->numy != 1 || cfg->m0 != 0 || cfg->precision != OSHUN_FP64 || !cfg->if_tridiagonal ||
-        ((cfg->nump + 31) / 32) * 32 > 256) {
-        set_error("the adjoint covers 1D runs (numy = 1) with m0 = 0, FP64, tridiagonal collisions, nump <= 256");
+    if (cfg->numy != 1 || cfg->m0 != 0 || !cfg->if_tridiagonal || ((cfg->nump + 31) / 32) * 32 > 256) {
+        set_error("the adjoint covers 1D runs (numy = 1) with m0 = 0, tridiagonal collisions, nump <= 256");
         return OSHUN_ERR_UNSUPPORTED;
     }
     if (cfg->flags & OSHUN_FLAG_IMPLICIT_EE) {
@@ -2103,6 +2116,8 @@ int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out) {
     int rc = oshun_create(cfg, &a->h);
     if (rc) { delete a; return rc; }
     oshun_ctx* h = a->h;
+    // FP32 bulk: the handle's planes hold f itself (the trajectory comes in as FP64 vectors)
+    h->use_profile = false;
     a->n = (1 + (long long)h->nplanes) * h->pstride + 6 * h->cells;
     auto fail = [&](int code) { free_adj(a); return code; };
     double** bufs[] = {&a->s2, &a->s3, &a->s4, &a->y1, &a->lam1, &a->c, &a->a, &a->acc};
@@ -2204,7 +2219,7 @@ int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, 
     for (int st = 3; st >= 0; --st) {
         if (st == 3) CK(launch_rk_combine(a->c, a->lam1, w_out[3], a->lam1, 0.0, nullptr, 0.0, n, h->stream));
         else CK(launch_rk_combine(a->c, a->lam1, w_out[st], a->a, w_in[st + 1], nullptr, 0.0, n, h->stream));
-        CK(launch_stage_vjp(g, S[st], a->c, a->a, h->stream));
+        CK(launch_stage_vjp(g, S[st], a->c, a->a, h->stream, h->fp32));
         CK(launch_rk_combine(a->acc, a->acc, 1.0, a->a, 1.0, nullptr, 0.0, n, h->stream));
     }
     CK(cudaMemcpyAsync(lam, a->acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));

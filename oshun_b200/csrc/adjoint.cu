@@ -1,6 +1,7 @@
 // Adjoint kernels of one small step of the 1D path with m0 = 0 (FP64), over
 // the math of adjoint_math.h:
-//   stage_vjp_kernel   F'(s)^T c for one RK4 stage state s: one CTA per cell,
+//   stage_vjp_kernel   F'(s)^T c for one RK4 stage state s (FP64 or FP32
+//                      arithmetic on FP64 vectors): one CTA per cell,
 //                      one thread per momentum point computes the cotangent
 //                      of every f_l(x, p) (transposed G/H stencils, x
 //                      advection, current) and its share of the E_x(x)
@@ -27,6 +28,9 @@ using adj::Coef1;
 using adj::CollTables;
 using adj::Grid1;
 
+// T: arithmetic of the transpose (double; float for the FP32 bulk form),
+// the vectors stay FP64
+template <typename T>
 __global__ void stage_vjp_kernel(const Grid1 g, const double* __restrict__ s, const double* __restrict__ c,
                                  double* __restrict__ out) {
     const int x = blockIdx.x;
@@ -38,8 +42,8 @@ __global__ void stage_vjp_kernel(const Grid1 g, const double* __restrict__ s, co
     double e = 0.0;
     if (k < g.np) {
         for (int l = 0; l <= g.l0; ++l)
-            out[((long long)l * g.nx + x) * g.np + k] = adj::vjp_f(g, Ex, c, cE, l, x, k);
-        e = adj::vjp_E_point(g, s, c, x, k);
+            out[((long long)l * g.nx + x) * g.np + k] = (double)adj::vjp_f<T>(g, Ex, c, cE, l, x, k);
+        e = (double)adj::vjp_E_point<T>(g, s, c, x, k);
     }
     // E_x cotangent: warp sums, then warps in order
     for (int off = 16; off > 0; off >>= 1) e += __shfl_xor_sync(0xffffffffu, e, off);
@@ -51,6 +55,16 @@ __global__ void stage_vjp_kernel(const Grid1 g, const double* __restrict__ s, co
         out[fsz + x] = tot;
         for (int f = 1; f < 6; ++f) out[fsz + (long long)f * g.nx + x] = 0.0;
     }
+}
+
+// FP64 state vector <-> the FP32 planes and fields of an FP32-split handle
+__global__ void to_fp32_kernel(const double* __restrict__ src, float* __restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+__global__ void to_fp64_kernel(const float* __restrict__ src, double* __restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
 }
 
 __global__ void __launch_bounds__(32) collide_adj_kernel(const CollTables T, const int l0, const double* __restrict__ y,
@@ -78,10 +92,27 @@ __global__ void rk_combine_kernel(double* out, const double* v0, double a0, cons
 
 }  // namespace
 
-cudaError_t launch_stage_vjp(const Grid1& g, const double* s, const double* c, double* out, cudaStream_t st) {
+cudaError_t launch_stage_vjp(const Grid1& g, const double* s, const double* c, double* out, cudaStream_t st,
+                             bool fp32) {
     const int threads = ((g.np + 31) / 32) * 32;
     if (threads > 256) return cudaErrorInvalidValue;
-    stage_vjp_kernel<<<g.nx, threads, 0, st>>>(g, s, c, out);
+    if (fp32) stage_vjp_kernel<float><<<g.nx, threads, 0, st>>>(g, s, c, out);
+    else stage_vjp_kernel<double><<<g.nx, threads, 0, st>>>(g, s, c, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(const double* src, float* dst, long long n, cudaStream_t st) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    if (b < 1) return cudaSuccess;
+    to_fp32_kernel<<<(unsigned)b, 256, 0, st>>>(src, dst, n);
+    return cudaGetLastError();
+}
+cudaError_t launch_convert(const float* src, double* dst, long long n, cudaStream_t st) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    if (b < 1) return cudaSuccess;
+    to_fp64_kernel<<<(unsigned)b, 256, 0, st>>>(src, dst, n);
     return cudaGetLastError();
 }
 

@@ -38,66 +38,75 @@ struct Coef1 {
 };
 
 // ---------------------------------------------------------------------------
-// momentum stencils: weight of f(k) in G_l(p) and H_l(p)
+// momentum stencils: weight of f(k) in G_l(p) and H_l(p).  T is the
+// arithmetic type of the stage transpose (double; float for the FP32 bulk
+// form); the data stay FP64 and are rounded to T where they are read.
 // ---------------------------------------------------------------------------
 // G for l >= 1 (0 at p = 0), dr = f(p-1) - f(p+1) with the reference's ends
-OSHUN_HD inline double wG(int p, int k, int np, double ipx, double gfac) {
-    if (p == 0) return 0.0;
+template <typename T = double>
+OSHUN_HD inline T wG(int p, int k, int np, T ipx, T gfac) {
+    if (p == 0) return T(0);
     if (p < np - 1) {
-        if (k == p - 1) return 1.0 + gfac;
-        if (k == p + 1) return -(1.0 + gfac);
+        if (k == p - 1) return T(1) + gfac;
+        if (k == p + 1) return -(T(1) + gfac);
         if (k == p) return ipx;
-        return 0.0;
+        return T(0);
     }
-    if (k == p - 1) return 1.0 + gfac;
-    if (k == p) return ipx - (1.0 + gfac);
-    return 0.0;
+    if (k == p - 1) return T(1) + gfac;
+    if (k == p) return ipx - (T(1) + gfac);
+    return T(0);
 }
 // H for l >= 1: H(0) = hp0 f(1)
-OSHUN_HD inline double wH(int p, int k, int np, double ipx, double hp0) {
-    if (p == 0) return k == 1 ? hp0 : 0.0;
+template <typename T = double>
+OSHUN_HD inline T wH(int p, int k, int np, T ipx, T hp0) {
+    if (p == 0) return k == 1 ? hp0 : T(0);
     if (p < np - 1) {
-        if (k == p - 1) return 1.0;
-        if (k == p + 1) return -1.0;
+        if (k == p - 1) return T(1);
+        if (k == p + 1) return T(-1);
         if (k == p) return ipx;
-        return 0.0;
+        return T(0);
     }
-    if (k == p - 1) return 1.0;
-    if (k == p) return ipx - 1.0;
-    return 0.0;
+    if (k == p - 1) return T(1);
+    if (k == p) return ipx - T(1);
+    return T(0);
 }
 // G00 of f00: f(p-1) - f(p+1) with the reference's ends, the p = 0
 // extrapolation (f(1) - f00x) g00_gr, f00x = (f(0) - f(1) g00_s) g00_inv
-OSHUN_HD inline double wG00(int p, int k, int np, double g00_s, double g00_inv, double g00_gr) {
+template <typename T = double>
+OSHUN_HD inline T wG00(int p, int k, int np, T g00_s, T g00_inv, T g00_gr) {
     if (p == 0) {
         if (k == 0) return -g00_gr * g00_inv;
-        if (k == 1) return g00_gr * (1.0 + g00_inv * g00_s);
-        return 0.0;
+        if (k == 1) return g00_gr * (T(1) + g00_inv * g00_s);
+        return T(0);
     }
     if (p < np - 1) {
-        if (k == p - 1) return 1.0;
-        if (k == p + 1) return -1.0;
-        return 0.0;
+        if (k == p - 1) return T(1);
+        if (k == p + 1) return T(-1);
+        return T(0);
     }
-    if (k == p - 1) return 1.0;
-    if (k == p) return -1.0;
-    return 0.0;
+    if (k == p - 1) return T(1);
+    if (k == p) return T(-1);
+    return T(0);
 }
 
 // the stencils applied to one row f[0..np)
-OSHUN_HD inline double applyG(const double* f, int p, int np, double ipx, double gfac) {
-    double s = 0.0;
-    for (int k = (p > 0 ? p - 1 : 0); k <= (p + 1 < np ? p + 1 : np - 1); ++k) s += wG(p, k, np, ipx, gfac) * f[k];
+template <typename T = double>
+OSHUN_HD inline T applyG(const double* f, int p, int np, T ipx, T gfac) {
+    T s = T(0);
+    for (int k = (p > 0 ? p - 1 : 0); k <= (p + 1 < np ? p + 1 : np - 1); ++k) s += wG<T>(p, k, np, ipx, gfac) * (T)f[k];
     return s;
 }
-OSHUN_HD inline double applyH(const double* f, int p, int np, double ipx, double hp0) {
-    double s = 0.0;
-    for (int k = (p > 0 ? p - 1 : 0); k <= (p + 1 < np ? p + 1 : np - 1); ++k) s += wH(p, k, np, ipx, hp0) * f[k];
+template <typename T = double>
+OSHUN_HD inline T applyH(const double* f, int p, int np, T ipx, T hp0) {
+    T s = T(0);
+    for (int k = (p > 0 ? p - 1 : 0); k <= (p + 1 < np ? p + 1 : np - 1); ++k) s += wH<T>(p, k, np, ipx, hp0) * (T)f[k];
     return s;
 }
-OSHUN_HD inline double applyG00(const double* f, int p, int np, double gs, double gi, double gg) {
-    double s = 0.0;
-    for (int k = (p > 0 ? p - 1 : 0); k <= (p + 1 < np ? p + 1 : np - 1); ++k) s += wG00(p, k, np, gs, gi, gg) * f[k];
+template <typename T = double>
+OSHUN_HD inline T applyG00(const double* f, int p, int np, T gs, T gi, T gg) {
+    T s = T(0);
+    for (int k = (p > 0 ? p - 1 : 0); k <= (p + 1 < np ? p + 1 : np - 1); ++k)
+        s += wG00<T>(p, k, np, gs, gi, gg) * (T)f[k];
     return s;
 }
 
@@ -146,56 +155,57 @@ OSHUN_HD inline void rhs_point(const Grid1& g, const double* f, const double* Ex
 
 // cotangent of f_s(x, k) from the slope cotangents cf[t][x][p] (masked
 // points carry no cotangent) and the E_x slope cotangent cE[x]
-OSHUN_HD inline double vjp_f(const Grid1& g, const double* Ex, const double* cf, const double* cE, int s, int x,
-                             int k) {
+template <typename T = double>
+OSHUN_HD inline T vjp_f(const Grid1& g, const double* Ex, const double* cf, const double* cE, int s, int x, int k) {
     const int np = g.np, nx = g.nx;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     const Coef1& c = g.coef[s];
-    const double E = Ex[x];
-    double acc = 0.0;
+    const T E = (T)Ex[x];
+    T acc = T(0);
     const int plo = k > 0 ? k - 1 : 0, phi = k + 1 < np ? k + 1 : np - 1;
     if (s + 1 <= g.l0) {   // source of target s+1 through G and x advection
         const int t = s + 1;
         const double* ct = row(cf, g, t, x);
         for (int p = plo; p <= phi; ++p) {
             if (clean_masked(t, p)) continue;
-            const double w = s == 0 ? wG00(p, k, np, g.g00_s, g.g00_inv, g.g00_gr)
-                                    : wG(p, k, np, g.invp[p] * c.invpax, c.gfac);
-            acc += E * c.ex_g * w * ct[p];
+            const T w = s == 0 ? wG00<T>(p, k, np, (T)g.g00_s, (T)g.g00_inv, (T)g.g00_gr)
+                               : wG<T>(p, k, np, (T)(g.invp[p] * c.invpax), (T)c.gfac);
+            acc += E * (T)c.ex_g * w * (T)ct[p];
         }
-        const double cxp = clean_masked(t, k) ? 0.0 : row(cf, g, t, xp)[k];
-        const double cxm = clean_masked(t, k) ? 0.0 : row(cf, g, t, xm)[k];
-        acc += c.ax_p * g.vr[k] * (cxp - cxm);
+        const T cxp = clean_masked(t, k) ? T(0) : (T)row(cf, g, t, xp)[k];
+        const T cxm = clean_masked(t, k) ? T(0) : (T)row(cf, g, t, xm)[k];
+        acc += (T)c.ax_p * (T)g.vr[k] * (cxp - cxm);
     }
     if (s >= 1) {          // source of target s-1 through H and x advection
         const int t = s - 1;
         const double* ct = row(cf, g, t, x);
         for (int p = plo; p <= phi; ++p) {
             if (clean_masked(t, p)) continue;
-            acc += E * c.ex_h * wH(p, k, np, g.invp[p] * c.invpax, c.hp0) * ct[p];
+            acc += E * (T)c.ex_h * wH<T>(p, k, np, (T)(g.invp[p] * c.invpax), (T)c.hp0) * (T)ct[p];
         }
-        const double cxp = clean_masked(t, k) ? 0.0 : row(cf, g, t, xp)[k];
-        const double cxm = clean_masked(t, k) ? 0.0 : row(cf, g, t, xm)[k];
-        acc += c.ax_m * g.vr[k] * (cxp - cxm);
+        const T cxp = clean_masked(t, k) ? T(0) : (T)row(cf, g, t, xp)[k];
+        const T cxm = clean_masked(t, k) ? T(0) : (T)row(cf, g, t, xm)[k];
+        acc += (T)c.ax_m * (T)g.vr[k] * (cxp - cxm);
     }
-    if (s == 1) acc += g.wj[k] * cE[x];
+    if (s == 1) acc += (T)g.wj[k] * (T)cE[x];
     return acc;
 }
 
 // one momentum point's share of the E_x(x) cotangent
-OSHUN_HD inline double vjp_E_point(const Grid1& g, const double* f, const double* cf, int x, int p) {
+template <typename T = double>
+OSHUN_HD inline T vjp_E_point(const Grid1& g, const double* f, const double* cf, int x, int p) {
     const int np = g.np;
-    double acc = 0.0;
+    T acc = T(0);
     for (int s = 0; s <= g.l0; ++s) {
         const Coef1& c = g.coef[s];
         const double* fr = row(f, g, s, x);
         if (s + 1 <= g.l0 && !clean_masked(s + 1, p)) {
-            const double G = s == 0 ? applyG00(fr, p, np, g.g00_s, g.g00_inv, g.g00_gr)
-                                    : applyG(fr, p, np, g.invp[p] * c.invpax, c.gfac);
-            acc += c.ex_g * G * row(cf, g, s + 1, x)[p];
+            const T G = s == 0 ? applyG00<T>(fr, p, np, (T)g.g00_s, (T)g.g00_inv, (T)g.g00_gr)
+                               : applyG<T>(fr, p, np, (T)(g.invp[p] * c.invpax), (T)c.gfac);
+            acc += (T)c.ex_g * G * (T)row(cf, g, s + 1, x)[p];
         }
         if (s >= 1 && !clean_masked(s - 1, p))
-            acc += c.ex_h * applyH(fr, p, np, g.invp[p] * c.invpax, c.hp0) * row(cf, g, s - 1, x)[p];
+            acc += (T)c.ex_h * applyH<T>(fr, p, np, (T)(g.invp[p] * c.invpax), (T)c.hp0) * (T)row(cf, g, s - 1, x)[p];
     }
     return acc;
 }

@@ -173,7 +173,11 @@ int collide_max_chunk(int np, size_t smem_budget);
 int collide_threads();
 size_t collide_tri_smem_per_cell(int np, int l0);
 // adjoint kernels of the 1D m0 = 0 step (adjoint.cu; types in adjoint_math.h)
-cudaError_t launch_stage_vjp(const adj::Grid1& g, const double* s, const double* c, double* out, cudaStream_t st);
+cudaError_t launch_stage_vjp(const adj::Grid1& g, const double* s, const double* c, double* out, cudaStream_t st,
+                             bool fp32);
+// FP64 state vector <-> FP32 planes/fields (the FP32 bulk adjoint)
+cudaError_t launch_convert(const double* src, float* dst, long long n, cudaStream_t st);
+cudaError_t launch_convert(const float* src, double* dst, long long n, cudaStream_t st);
 cudaError_t launch_collide_adj(const adj::CollTables& T, int l0, int nx, const double* y, double* lam, int ee, int eb,
                                int nsub, double hsub, double Dt, double* ws, long long wsz, cudaStream_t st);
 cudaError_t launch_rk_combine(double* out, const double* v0, double a0, const double* v1, double a1, const double* v2,
