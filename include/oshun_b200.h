@@ -134,6 +134,48 @@ int oshun_collide_flm(oshun_handle h, double t_new);
  * CUDA graph once captured.  `collisions` = 0 skips the collision calls. */
 int oshun_step(oshun_handle h, int nsteps, int collisions);
 
+/* ---- x boundaries and x slabs -------------------------------------------- */
+
+/* The reference's x boundary of a grid (input deck bndX, OSHUN-1/
+ * def-Parallel.cpp:1115-1135) and its split over ranks in x
+ * (Parallel_Environment::Neighbor_Communications, :3040-3129):
+ *   OSHUN_XB_PERIODIC  (default) sameNode_periodic_X, :1138-1158;
+ *   OSHUN_XB_MIRROR    sameNode_mirror_X (:1160-1206): the guard next to an
+ *                      edge column is that column, times (-1)^(l+m) on f_lm
+ *                      and -1 on Ey, Ez and Bx (every l; the reference leaves
+ *                      the l = l0 guards as they are);
+ *   OSHUN_XB_HALO      the grid is one x slab of a larger grid: the x-1
+ *                      neighbour of column 0 and the x+1 neighbour of column
+ *                      numx-1 are halo columns the caller loads before every
+ *                      RK4 stage (oshun_halo_pack on each rank, the exchange
+ *                      with the left and right ranks, oshun_halo_unpack), and
+ *                      the step runs stage by stage (oshun_step_stage).
+ * FP64 only for MIRROR and HALO; y stays periodic. */
+#define OSHUN_XB_PERIODIC 0
+#define OSHUN_XB_MIRROR 1
+#define OSHUN_XB_HALO 2
+int oshun_set_x_boundary(oshun_handle h, int mode);
+/* bytes of one halo column set (one edge column: f00 [numy][nump] FP64, the
+ * l >= 1 planes [nplanes][numy][nump], the fields [6][numy], each part
+ * 256-byte aligned) */
+int oshun_halo_bytes(oshun_handle h, long long* bytes);
+/* the next stage's input columns x = 0 -> left_edge and x = numx-1 ->
+ * right_edge (device buffers of oshun_halo_bytes each; the left one goes to
+ * the left neighbour, the right one to the right neighbour) */
+int oshun_halo_pack(oshun_handle h, void* left_edge, void* right_edge);
+/* the neighbours' columns: from_left = the left rank's right_edge, from_right
+ * = the right rank's left_edge (device buffers) */
+int oshun_halo_unpack(oshun_handle h, const void* from_left, const void* from_right);
+/* the halo of side 0 (left) or 1 (right) as a mirrored boundary of the next
+ * stage's input (the end ranks of a slab split with bndX = 1:
+ * Node_Communications::mirror_bound_Xleft/right, def-Parallel.cpp:964-1031,
+ * called at :3058, 3075) */
+int oshun_halo_mirror_side(oshun_handle h, int side);
+/* RK4 stage k (1..4, in order) of the small step; stage 4 completes the RK4
+ * step (Runge_Kutta_4::advance_p1) and, with `collisions`, runs the e-e and
+ * implicit f_lm steps of oshun_step. */
+int oshun_step_stage(oshun_handle h, int k, int collisions);
+
 /* nsteps of the reference's small step with the implicit electric field
  * (OSHUN-1/main.cpp:77-107 with implicit_E; Runge_Kutta_2_Imp, def-RK.cpp:
  * 399-588; Implicit_E_Field, def-ImplicitE.cpp:471-676), cfg.dt the RK2 step h.

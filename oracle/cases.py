@@ -228,6 +228,7 @@ class Oracle:
         self.lib.oo_steps.argtypes = [ctypes.POINTER(_OoDeck), dp, ctypes.c_int, ctypes.c_int]
         self.lib.oo_set_yadv_chain.argtypes = [ctypes.c_int]
         self.lib.oo_set_ee_implicit.argtypes = [ctypes.c_int]
+        self.lib.oo_set_mirror_x.argtypes = [ctypes.c_int]
         self.lib.oo_nondominant_count.restype = ctypes.c_long
 
     @staticmethod
@@ -258,6 +259,10 @@ class Oracle:
         """0: the reference's explicit e-e substeps; > 0: the opt-in
         backward-Euler e-e step with that many Picard sweeps."""
         self.lib.oo_set_ee_implicit(int(sweeps))
+
+    def set_mirror_x(self, on: bool) -> None:
+        """mirrored (True) or periodic (False, default) x boundaries"""
+        self.lib.oo_set_mirror_x(1 if on else 0)
 
     def nondominant(self) -> int:
         return int(self.lib.oo_nondominant_count())

@@ -28,6 +28,11 @@ static int g_keep_chain = 1;
 static long g_nondominant = 0;
 
 void oo_set_yadv_chain(int keep) { g_keep_chain = keep ? 1 : 0; }
+/* mirrored x boundaries (Node_Communications::sameNode_mirror_X,
+ * def-Parallel.cpp:1160-1206): the neighbour beyond an edge column is that
+ * column, times (-1)^(l+m) on f_lm and -1 on Ey, Ez, Bx (every l) */
+static int g_mirror_x = 0;
+void oo_set_mirror_x(int on) { g_mirror_x = on ? 1 : 0; }
 long oo_nondominant_count(void) { return g_nondominant; }
 
 /* ------------------------------------------------------------------------ */
@@ -264,8 +269,12 @@ static void rhs(const Grid* g, const cplx* Y, cplx* S) {
                 const cplx ex = Ex[c], em = Ey[c] - I * Ez[c], ep = Ey[c] + I * Ez[c];
                 const cplx bx = Bx[c], bm = Bz[c] - I * By[c], bp = (Bz[c] + I * By[c]) * 0.5;
                 /* advection neighbours */
-                const cplx* fxm = f + cell_xm(g, c) * np;
-                const cplx* fxp = f + cell_xp(g, c) * np;
+                const long xc = c % g->nx;
+                const double sgn = ((l + m) & 1) ? -1.0 : 1.0;
+                const int mxm = g_mirror_x && xc == 0, mxp = g_mirror_x && xc == g->nx - 1;
+                const cplx* fxm = f + (mxm ? c : cell_xm(g, c)) * np;
+                const cplx* fxp = f + (mxp ? c : cell_xp(g, c)) * np;
+                const double sxm = mxm ? sgn : 1.0, sxp = mxp ? sgn : 1.0;
                 const cplx* fym = f + cell_ym(g, c) * np;
                 const cplx* fyp = f + cell_yp(g, c) * np;
                 const double qy = yadv_factor(g, l, m);
@@ -293,7 +302,7 @@ static void rhs(const Grid* g, const cplx* Y, cplx* S) {
                     else if (m >= 2) addto(S, g, l, m - 1, k, (-0.5 * (l + 1.0 - m) * (l + m)) * bm * fv);
                     /* x advection (def-VlasovMax.cpp:842-853), Dx f = f[x-1]-f[x+1]
                      * (matrices.h:813-820) */
-                    const cplx dxf = (fxm[p] - fxp[p]) * g->vr[p];
+                    const cplx dxf = (sxm * fxm[p] - sxp * fxp[p]) * g->vr[p];
                     if (l < g->l0) addto(S, g, l + 1, m, k, xA1(g, l, m) * dxf);
                     if (l >= 1 && l - 1 >= m) addto(S, g, l - 1, m, k, xA2(g, l, m) * dxf);
                     /* y advection (def-VlasovMax.cpp:857-947) */
@@ -357,16 +366,20 @@ static void rhs(const Grid* g, const cplx* Y, cplx* S) {
     /* Ampere and Faraday, MaxwellEq (def-VlasovMax.cpp:979-1035):
      * idx*Dx g = (g[x+1]-g[x-1])/(2dx) */
     for (long c = 0; c < cells; ++c) {
-        const long xm = cell_xm(g, c), xp = cell_xp(g, c), ym = cell_ym(g, c), yp = cell_yp(g, c);
+        const long ym = cell_ym(g, c), yp = cell_yp(g, c);
+        const long xc = c % g->nx;
+        const int mxm = g_mirror_x && xc == 0, mxp = g_mirror_x && xc == g->nx - 1;
+        const long xm = mxm ? c : cell_xm(g, c), xp = mxp ? c : cell_xp(g, c);
+        const double sm = mxm ? -1.0 : 1.0, sp = mxp ? -1.0 : 1.0;   /* Ey, Ez flip at a mirror */
         cplx dEx = 0, dEy = 0, dEz = 0, dBx = 0, dBy = 0, dBz = 0;
         dEx += g->idy * (Bz[ym] - Bz[yp]);
         dEy += -g->idx * (Bz[xm] - Bz[xp]);
         dEz += -g->idy * (Bx[ym] - Bx[yp]);
         dEz += g->idx * (By[xm] - By[xp]);
         dBx += -g->idy * (Ez[ym] - Ez[yp]);
-        dBy += g->idx * (Ez[xm] - Ez[xp]);
+        dBy += g->idx * (sm * Ez[xm] - sp * Ez[xp]);
         dBz += g->idy * (Ex[ym] - Ex[yp]);
-        dBz += -g->idx * (Ey[xm] - Ey[xp]);
+        dBz += -g->idx * (sm * Ey[xm] - sp * Ey[xp]);
         dF[c] += dEx; dF[cells + c] += dEy; dF[2 * cells + c] += dEz;
         dF[3 * cells + c] += dBx; dF[4 * cells + c] += dBy; dF[5 * cells + c] += dBz;
     }

@@ -35,6 +35,10 @@ void oo_set_yadv_chain(int keep);
  * sweeps (OSHUN_FLAG_IMPLICIT_EE of the CUDA path) */
 void oo_set_ee_implicit(int sweeps);
 
+/* x boundaries of later calls: 0 periodic (default), 1 mirrored
+ * (sameNode_mirror_X: (-1)^(l+m) on f_lm, -1 on Ey, Ez, Bx, every l) */
+void oo_set_mirror_x(int on);
+
 long oo_state_doubles(const oo_deck* d);
 
 /* slope = Actions::Adv(state) */

@@ -35,7 +35,10 @@ EXPORTED = [
     "oshun_adjoint_forward", "oshun_adjoint_vjp", "oshun_debug_inject_stage_timeout", "oshun_get_config",
     "oshun_moments", "oshun_restart_bytes", "oshun_restart_pack", "oshun_restart_unpack", "oshun_restart_write",
     "oshun_restart_read", "oshun_rk2_imp_step", "oshun_plane_profile",
+    "oshun_set_x_boundary", "oshun_halo_bytes", "oshun_halo_pack", "oshun_halo_unpack", "oshun_halo_mirror_side",
+    "oshun_step_stage",
 ]
+OSHUN_XB_PERIODIC, OSHUN_XB_MIRROR, OSHUN_XB_HALO = 0, 1, 2
 
 
 class OshunCfg(ctypes.Structure):
@@ -91,6 +94,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.oshun_debug_inject_stage_timeout.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     lib.oshun_get_config.argtypes = [vp, ctypes.POINTER(OshunCfg)]
     lib.oshun_rk2_imp_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.oshun_set_x_boundary.argtypes = [vp, ctypes.c_int]
+    lib.oshun_halo_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.oshun_halo_pack.argtypes = [vp, vp, vp]
+    lib.oshun_halo_unpack.argtypes = [vp, vp, vp]
+    lib.oshun_step_stage.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.oshun_halo_mirror_side.argtypes = [vp, ctypes.c_int]
     lib.oshun_plane_profile.argtypes = [vp, ctypes.POINTER(vp)]
     lib.oshun_moments.argtypes = [vp, vp]
     lib.oshun_restart_bytes.argtypes = [ctypes.POINTER(OshunCfg), ctypes.c_int]
@@ -227,6 +236,31 @@ class Handle:
     def rk2_imp_step(self, nsteps: int, mask: int = 63) -> None:
         """nsteps of the implicit-E small step (mask bits as oshun_rk2_imp_step)."""
         self._check(self.lib.oshun_rk2_imp_step(self._h, nsteps, mask), "oshun_rk2_imp_step")
+
+    def set_x_boundary(self, mode: int) -> None:
+        """OSHUN_XB_PERIODIC, OSHUN_XB_MIRROR or OSHUN_XB_HALO (an x slab)."""
+        self._check(self.lib.oshun_set_x_boundary(self._h, int(mode)), "oshun_set_x_boundary")
+
+    def halo_bytes(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self.lib.oshun_halo_bytes(self._h, ctypes.byref(n)), "oshun_halo_bytes")
+        return n.value
+
+    def halo_pack(self, left_edge: int, right_edge: int) -> None:
+        """The next stage's edge columns into two device buffers (pointers)."""
+        self._check(self.lib.oshun_halo_pack(self._h, left_edge, right_edge), "oshun_halo_pack")
+
+    def halo_unpack(self, from_left: int, from_right: int) -> None:
+        """The neighbours' edge columns (device pointers) into the halo."""
+        self._check(self.lib.oshun_halo_unpack(self._h, from_left, from_right), "oshun_halo_unpack")
+
+    def halo_mirror_side(self, side: int) -> None:
+        """Side 0 (left) or 1 (right) of the halo as a mirrored boundary."""
+        self._check(self.lib.oshun_halo_mirror_side(self._h, int(side)), "oshun_halo_mirror_side")
+
+    def step_stage(self, k: int, collisions: bool = True) -> None:
+        """RK4 stage k (1..4) of the small step; stage 4 also collides."""
+        self._check(self.lib.oshun_step_stage(self._h, int(k), int(bool(collisions))), "oshun_step_stage")
 
     def synchronize(self) -> None:
         self._check(self.lib.oshun_synchronize(self._h), "oshun_synchronize")

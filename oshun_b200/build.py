@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "liboshun_b200.so")
 SOURCES = ["vlasov.cu", "stage_pipe.cu", "stage_batch.cu", "collide.cu", "adjoint.cu", "abi.cu", "noalloc.cu",
-           "moments.cu", "restart.cu", "implicit_e.cu"]
+           "moments.cu", "restart.cu", "implicit_e.cu", "halo.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -274,6 +274,11 @@ struct oshun_ctx {
     bool imp_zero_seen = false;  // some implicit-E solve since the last status read left one
     double* d_mom_tab = nullptr; // moments: p, 1/gamma, pow tables [7][np] (built on first use)
     float* d_mom = nullptr;      // moments: [kMomCount + 1][cells] (the last plane is scratch)
+    // x boundary (OSHUN_XB_*) and the x halo column sets of the next stage's input
+    int xb = 0;
+    unsigned char* d_hx = nullptr;
+    long long hx_side = 0, hx_pl = 0, hx_fld = 0;
+    int stage_next = 1;          // the RK4 stage oshun_step_stage runs next (1..4)
 
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -384,6 +389,7 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     std::memset(&a, 0, sizeof(a));
     a.f00_in = f00[in_set]; a.pl_in = (const TS*)pl[in_set]; a.fld_in = (const TS*)fld[in_set];
     a.pl_ref = use_profile ? (const TS*)d_ref_ts : nullptr;
+    if (xb != OSHUN_XB_PERIODIC) { a.hx = d_hx; a.hx_side = hx_side; a.hx_pl = hx_pl; a.hx_fld = hx_fld; }
     a.coef = d_coef; a.plane_of = d_plane_of;
     a.inv_pr = d_ptab; a.vr = d_ptab + cfg.nump; a.wj = d_ptab + 2 * cfg.nump;
     a.cells = cells; a.pstride = pstride;
@@ -594,15 +600,45 @@ int launch_stage(oshun_ctx* h, int in_set, int B_set, int A_set, int out_set, in
     return OSHUN_OK;
 }
 
-// Runge_Kutta_4::advance_p1 (def-RK.cpp:116-142) on set cur -> set nxt
-int enqueue_rk4(oshun_ctx* h) {
+HaloGrid halo_grid(const oshun_ctx* h) {
+    HaloGrid g;
+    g.nx = h->cfg.numx; g.ny = h->cfg.numy; g.np = h->cfg.nump; g.nplanes = h->nplanes;
+    g.pstride = h->pstride; g.cells = h->cells;
+    g.off_pl = h->hx_pl; g.off_fld = h->hx_fld;
+    g.plane_l = h->d_plane_l; g.plane_m = h->d_plane_m;
+    return g;
+}
+
+// the halo columns of set `set` from its own edge columns: mirrored x
+// boundaries (sameNode_mirror_X, def-Parallel.cpp:1160-1206)
+int fill_mirror(oshun_ctx* h, int set) {
+    if (h->xb != OSHUN_XB_MIRROR) return OSHUN_OK;
+    CK(launch_halo_columns(h->f00[set], h->pl[set], h->fld[set], halo_grid(h), h->fp32, h->d_hx,
+                           h->d_hx + h->hx_side, 1, h->stream));
+    return OSHUN_OK;
+}
+
+// RK4 stage k (1..4) of Runge_Kutta_4::advance_p1 (def-RK.cpp:116-142) on set
+// cur: inputs cur, Sa, Sb, Sa; the fourth writes the step's result to cur ^ 1
+int stage_input(const oshun_ctx* h, int k) { return k == 1 ? h->cur : (k == 3 ? 3 : 2); }
+int enqueue_stage(oshun_ctx* h, int k) {
     const double dt = h->cfg.dt;
     const int B = h->cur, A = h->cur ^ 1, Sa = 2, Sb = 3;
+    int rc = fill_mirror(h, stage_input(h, k));
+    if (rc) return rc;
+    switch (k) {
+        case 1: return launch_stage(h, B, B, A, Sa, 0, 1, 0.5 * dt, 1.0 / 3.0);
+        case 2: return launch_stage(h, Sa, B, A, Sb, 0, 0, 0.5 * dt, 2.0 / 3.0);
+        case 3: return launch_stage(h, Sb, B, A, Sa, 0, 0, dt, 1.0 / 3.0);
+        default: return launch_stage(h, Sa, B, A, -1, 0, 0, dt / 6.0, 1.0);
+    }
+}
+
+// Runge_Kutta_4::advance_p1 on set cur -> set cur ^ 1
+int enqueue_rk4(oshun_ctx* h) {
     int rc;
-    if ((rc = launch_stage(h, B, B, A, Sa, 0, 1, 0.5 * dt, 1.0 / 3.0))) return rc;   // k1
-    if ((rc = launch_stage(h, Sa, B, A, Sb, 0, 0, 0.5 * dt, 2.0 / 3.0))) return rc;  // k2
-    if ((rc = launch_stage(h, Sb, B, A, Sa, 0, 0, dt, 1.0 / 3.0))) return rc;        // k3
-    if ((rc = launch_stage(h, Sa, B, A, -1, 0, 0, dt / 6.0, 1.0))) return rc;         // k4
+    for (int k = 1; k <= 4; ++k)
+        if ((rc = enqueue_stage(h, k))) return rc;
     return OSHUN_OK;
 }
 
@@ -879,7 +915,7 @@ void free_ctx(oshun_ctx* h) {
     cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
     cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage); cudaFree(h->d_jw);
     cudaFree(h->d_mom_tab); cudaFree(h->d_mom);
-    cudaFree(h->d_ref64); cudaFree(h->d_ref_ts); cudaFree(h->d_refpart);
+    cudaFree(h->d_ref64); cudaFree(h->d_ref_ts); cudaFree(h->d_refpart); cudaFree(h->d_hx);
     for (int i = 0; i < 4; ++i) cudaFree(h->d_coef_imp[i]);
     cudaFree(h->d_imp); cudaFree(h->d_fe); cudaFree(h->d_zeros);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1079,13 +1115,25 @@ int oshun_download(oshun_handle h, double* harmonics, double* fields) {
 int oshun_rhs(oshun_handle h, double* slope_harmonics, double* slope_fields) {
     if (!h || !slope_harmonics || !slope_fields) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
     // slope written to set 2 (scratch), in plane layout
-    int rc = launch_stage(h, h->cur, h->cur, h->cur, 2, 1, 0, 1.0, 1.0);
+    int rc = fill_mirror(h, h->cur);
+    if (rc) return rc;
+    rc = launch_stage(h, h->cur, h->cur, h->cur, 2, 1, 0, 1.0, 1.0);
     if (rc) return rc;
     return gather_to_host(h, 2, slope_harmonics, slope_fields, false);
 }
 
+static int refuse_halo(oshun_handle h) {
+    if (h->xb == OSHUN_XB_HALO) {
+        set_error("an x slab (OSHUN_XB_HALO) steps stage by stage: oshun_step_stage, with the halo "
+                  "columns loaded before each stage");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
+    return OSHUN_OK;
+}
+
 int oshun_rk4_step(oshun_handle h) {
     if (!h) return OSHUN_ERR_ARG;
+    if (int rc = refuse_halo(h)) return rc;
     h->inject_active = h->inject_armed;
     h->inject_armed = false;
     int rc = enqueue_rk4(h);
@@ -1133,6 +1181,7 @@ int oshun_collide_flm(oshun_handle h, double t_new) {
 
 int oshun_step(oshun_handle h, int nsteps, int collisions) {
     if (!h || nsteps < 0) return OSHUN_ERR_ARG;
+    if (int rc = refuse_halo(h)) return rc;
     collisions = collisions ? 1 : 0;
     Clock ck{h->t, h->t_ee, h->t_eb};
     CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
@@ -1173,8 +1222,107 @@ int oshun_step(oshun_handle h, int nsteps, int collisions) {
     return OSHUN_OK;
 }
 
+int oshun_set_x_boundary(oshun_handle h, int mode) {
+    if (!h) return OSHUN_ERR_ARG;
+    if (mode != OSHUN_XB_PERIODIC && mode != OSHUN_XB_MIRROR && mode != OSHUN_XB_HALO) {
+        set_error("x boundary: OSHUN_XB_PERIODIC, OSHUN_XB_MIRROR or OSHUN_XB_HALO");
+        return OSHUN_ERR_ARG;
+    }
+    if (mode != OSHUN_XB_PERIODIC && h->fp32) {
+        // FP32 planes hold deviations from this grid's own momentum profile
+        set_error("mirrored and slab x boundaries run in FP64");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
+    if (mode != OSHUN_XB_PERIODIC && !h->d_hx) {
+        const long long ts = h->fp32 ? 4 : 8;
+        auto al = [](long long b) { return (b + 255) / 256 * 256; };
+        const long long ny = h->cfg.numy, np = h->cfg.nump;
+        h->hx_pl = al(ny * np * 8);
+        h->hx_fld = h->hx_pl + al((long long)h->nplanes * ny * np * ts);
+        h->hx_side = h->hx_fld + al(6 * ny * ts);
+        CK(cudaMalloc(&h->d_hx, 2 * h->hx_side));
+        CK(cudaMemset(h->d_hx, 0, 2 * h->hx_side));
+    }
+    if (mode != h->xb) {
+        // the captured step graphs hold the old boundary's launches
+        CK(cudaStreamSynchronize(h->stream));
+        for (auto& row : h->graph)
+            for (auto& g : row)
+                if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+    h->xb = mode;
+    h->stage_next = 1;
+    return OSHUN_OK;
+}
+
+int oshun_halo_bytes(oshun_handle h, long long* bytes) {
+    if (!h || !bytes) return OSHUN_ERR_ARG;
+    if (h->xb == OSHUN_XB_PERIODIC) { set_error("periodic x boundaries have no halo columns"); return OSHUN_ERR_ARG; }
+    *bytes = h->hx_side;
+    return OSHUN_OK;
+}
+
+int oshun_halo_pack(oshun_handle h, void* left_edge, void* right_edge) {
+    if (!h || !left_edge || !right_edge) return OSHUN_ERR_ARG;
+    if (h->xb != OSHUN_XB_HALO) { set_error("oshun_halo_pack needs OSHUN_XB_HALO"); return OSHUN_ERR_ARG; }
+    const int set = stage_input(h, h->stage_next);
+    CK(launch_halo_columns(h->f00[set], h->pl[set], h->fld[set], halo_grid(h), h->fp32, left_edge, right_edge, 0,
+                           h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_halo_unpack(oshun_handle h, const void* from_left, const void* from_right) {
+    if (!h || !from_left || !from_right) return OSHUN_ERR_ARG;
+    if (h->xb != OSHUN_XB_HALO) { set_error("oshun_halo_unpack needs OSHUN_XB_HALO"); return OSHUN_ERR_ARG; }
+    CK(cudaMemcpyAsync(h->d_hx, from_left, h->hx_side, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->d_hx + h->hx_side, from_right, h->hx_side, cudaMemcpyDeviceToDevice, h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_halo_mirror_side(oshun_handle h, int side) {
+    if (!h || (side != 0 && side != 1)) return OSHUN_ERR_ARG;
+    if (h->xb != OSHUN_XB_HALO) { set_error("oshun_halo_mirror_side needs OSHUN_XB_HALO"); return OSHUN_ERR_ARG; }
+    const int set = stage_input(h, h->stage_next);
+    CK(launch_halo_column(h->f00[set], h->pl[set], h->fld[set], halo_grid(h), h->fp32,
+                          side == 0 ? 0 : h->cfg.numx - 1, h->d_hx + (side ? h->hx_side : 0), 1, h->stream));
+    return OSHUN_OK;
+}
+
+int oshun_step_stage(oshun_handle h, int k, int collisions) {
+    if (!h) return OSHUN_ERR_ARG;
+    if (k != h->stage_next) { set_error("stages run in order 1, 2, 3, 4"); return OSHUN_ERR_ARG; }
+    int rc = enqueue_stage(h, k);
+    if (rc) return rc;
+    if (k < 4) {
+        h->stage_next = k + 1;
+        CK(cudaStreamSynchronize(h->stream));
+        return OSHUN_OK;
+    }
+    h->stage_next = 1;
+    h->cur ^= 1;
+    h->t += h->cfg.dt;
+    clock_advance_kernel<<<1, 1, 0, h->stream>>>(h->d_clock, h->cfg.dt);
+    CK(cudaGetLastError());
+    if (collisions) {
+        int nsub; double hsub, Dt;
+        collide_params(h, h->t, &nsub, &hsub, &Dt);
+        if ((rc = enqueue_collide(h, 1, 1, 1, nsub, hsub, Dt))) return rc;
+        clock_commit_kernel<<<1, 1, 0, h->stream>>>(h->d_clock, 1, 1);
+        CK(cudaGetLastError());
+        h->t_ee = h->t;
+        h->t_eb = h->t;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    return OSHUN_OK;
+}
+
 int oshun_rk2_imp_step(oshun_handle h, int nsteps, int mask) {
     if (!h || nsteps < 0) return OSHUN_ERR_ARG;
+    if (h->xb != OSHUN_XB_PERIODIC) {
+        set_error("the implicit-E step runs with periodic x boundaries");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
     if (mask < 0 || mask > 63) { set_error("mask: bits 1, 2, 4, 8, 16, 32"); return OSHUN_ERR_ARG; }
     if (!h->d_imp) {
         const int rc = build_implicit(h);

@@ -87,7 +87,26 @@ struct StageArgs {
     int withhold;         // fault injection for tests: CTA 0's source producer skips this copy (-1: none)
     const void* coef_ts;  // coupling table in the arithmetic type (batched launches)
     double* jw;           // [cells][3][8]: per-warp partial sums of Jx, Re Jy, Im Jy (single-problem pipeline)
+    // x halo columns of the stage input (null: periodic in x).  Side 0 is the
+    // x-1 neighbour of column 0, side 1 the x+1 neighbour of column nx-1;
+    // one side (hx_side bytes apart): f00 [ny][np] FP64, at hx_pl the l >= 1
+    // planes [nplanes][ny][np], at hx_fld the fields [6][ny]
+    const unsigned char* hx;
+    long long hx_side, hx_pl, hx_fld;
 };
+
+template <typename TS>
+__device__ __forceinline__ const double* hx_f00(const StageArgs<TS>& a, int side, long long y) {
+    return reinterpret_cast<const double*>(a.hx + side * a.hx_side) + y * a.np;
+}
+template <typename TS>
+__device__ __forceinline__ const TS* hx_plane(const StageArgs<TS>& a, int side, long long q, long long y) {
+    return reinterpret_cast<const TS*>(a.hx + side * a.hx_side + a.hx_pl) + (q * a.ny + y) * a.np;
+}
+template <typename TS>
+__device__ __forceinline__ TS hx_field(const StageArgs<TS>& a, int side, int k, long long y) {
+    return reinterpret_cast<const TS*>(a.hx + side * a.hx_side + a.hx_fld)[(long long)k * a.ny + y];
+}
 
 struct CollideArgs {
     double* f00;          // FP64 f00 plane (in/out)
@@ -120,6 +139,21 @@ struct CollideArgs {
     const double* clock;
     double small_dt;
 };
+
+// x halo column sets (halo.cu): grid sizes and one side's layout
+struct HaloGrid {
+    int nx, ny, np, nplanes;
+    long long pstride, cells;
+    long long off_pl, off_fld;      // byte offsets of the planes and fields in one side
+    const int *plane_l, *plane_m;   // [nplanes]
+};
+// the edge columns x = 0 and x = nx-1 of one state set into side0 / side1
+// (times the mirror signs when `mirror`)
+cudaError_t launch_halo_columns(const double* f00, const void* pl, const void* fld, const HaloGrid& g, bool fp32,
+                                void* side0, void* side1, int mirror, cudaStream_t st);
+// one column x0 into one side's column set
+cudaError_t launch_halo_column(const double* f00, const void* pl, const void* fld, const HaloGrid& g, bool fp32,
+                               int x0, void* out, int mirror, cudaStream_t st);
 
 // opt-in backward-Euler e-e step (a.ee_implicit sweeps), one warp per cell
 cudaError_t launch_ee_implicit(const CollideArgs& a, cudaStream_t st);

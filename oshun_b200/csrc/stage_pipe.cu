@@ -105,9 +105,19 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                             if (x_contig) {
                                 bulk_g2s(cb, pb + (size_t)xm_cell * bpc, (txv + 2) * bpc, full + slot);
                             } else {
-                                bulk_g2s(cb, pb + (size_t)xm_cell * bpc, bpc, full + slot);
+                                // the edge neighbours come from the x halo columns when the
+                                // grid has them (an x slab, or mirrored x boundaries)
+                                auto halo = [&](int side) -> const unsigned char* {
+                                    if (s == 0) return reinterpret_cast<const unsigned char*>(hx_f00(a, side, y));
+                                    const long long q = splane[s * mstride + m];
+                                    return reinterpret_cast<const unsigned char*>(hx_plane(a, side, q + comp, y));
+                                };
+                                const unsigned char* sxm = (a.hx && x0 == 0) ? halo(0) : pb + (size_t)xm_cell * bpc;
+                                const unsigned char* sxp =
+                                    (a.hx && x0 + txv == nx) ? halo(1) : pb + (size_t)xp_cell * bpc;
+                                bulk_g2s(cb, sxm, bpc, full + slot);
                                 bulk_g2s(cb + bpc, pb + (size_t)(row + x0) * bpc, txv * bpc, full + slot);
-                                bulk_g2s(cb + (size_t)(txv + 1) * bpc, pb + (size_t)xp_cell * bpc, bpc, full + slot);
+                                bulk_g2s(cb + (size_t)(txv + 1) * bpc, sxp, bpc, full + slot);
                             }
                             if (has_y) {
                                 bulk_g2s(cb + (size_t)(tx + 2) * bpc, pb + (size_t)(rym + x0) * bpc, txv * bpc,

@@ -402,23 +402,28 @@ __device__ __forceinline__ void couple_f00(AccF<MC>& A2, const CoefT<float>& c, 
 }
 
 // field epilogue: J reduction result + Ampere/Faraday, RK update of 6 fields
+// hside: bit 0 the x-1 neighbour, bit 1 the x+1 neighbour comes from the
+// x halo columns (row y)
 template <typename TS>
 __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long cell, long long cxm, long long cxp,
-                                             long long cym, long long cyp, double Jx, double Jyr, double Jyi) {
+                                             long long cym, long long cyp, double Jx, double Jyr, double Jyi,
+                                             int hside = 0, long long y = 0) {
     const TS* F = a.fld_in;
     const long long C = a.cells;
     const TS idx = (TS)a.idx, idy = (TS)a.idy;
+    auto xm = [&](int k) { return (hside & 1) ? hx_field(a, 0, k, y) : ldg(F + k * C + cxm); };
+    auto xp = [&](int k) { return (hside & 2) ? hx_field(a, 1, k, y) : ldg(F + k * C + cxp); };
     TS dEx = (TS)Jx;
     TS dEy = (TS)(2.0 * Jyr);
     TS dEz = (TS)(-(2.0 * Jyi));
     dEx += idy * (ldg(F + 5 * C + cym) - ldg(F + 5 * C + cyp));
-    dEy += -idx * (ldg(F + 5 * C + cxm) - ldg(F + 5 * C + cxp));
+    dEy += -idx * (xm(5) - xp(5));
     dEz += -idy * (ldg(F + 3 * C + cym) - ldg(F + 3 * C + cyp));
-    dEz += idx * (ldg(F + 4 * C + cxm) - ldg(F + 4 * C + cxp));
+    dEz += idx * (xm(4) - xp(4));
     TS dBx = -idy * (ldg(F + 2 * C + cym) - ldg(F + 2 * C + cyp));
-    TS dBy = idx * (ldg(F + 2 * C + cxm) - ldg(F + 2 * C + cxp));
+    TS dBy = idx * (xm(2) - xp(2));
     TS dBz = idy * (ldg(F + 0 * C + cym) - ldg(F + 0 * C + cyp));
-    dBz += -idx * (ldg(F + 1 * C + cxm) - ldg(F + 1 * C + cxp));
+    dBz += -idx * (xm(1) - xp(1));
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 0 * C + cell, dEx);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 1 * C + cell, dEy);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 2 * C + cell, dEz);
@@ -445,7 +450,8 @@ __device__ __forceinline__ void fields_cell(const StageArgs<TS>& a, const long l
     }
     const long long cxm = row + (xc == 0 ? nx - 1 : xc - 1);
     const long long cxp = row + (xc == nx - 1 ? 0 : xc + 1);
-    field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi);
+    const int hside = a.hx ? ((xc == 0 ? 1 : 0) | (xc == nx - 1 ? 2 : 0)) : 0;
+    field_update(a, cell, cxm, cxp, rym + xc, ryp + xc, Jx, Jyr, Jyi, hside, y);
 }
 
 // the field step of every problem of a batch: one CTA per problem

@@ -46,12 +46,17 @@ __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
 // ---------------------------------------------------------------------------
 // field epilogue: J reduction result + Ampere/Faraday, RK update of 6 fields
 // ---------------------------------------------------------------------------
+// hside: bit 0 the x-1 neighbour, bit 1 the x+1 neighbour comes from the
+// x halo columns (row y)
 template <typename TS>
 __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long cell, long long cxm, long long cxp,
-                                             long long cym, long long cyp, double Jx, double Jyr, double Jyi) {
+                                             long long cym, long long cyp, double Jx, double Jyr, double Jyi,
+                                             int hside, long long y) {
     const TS* F = a.fld_in;
     const long long C = a.cells;
     const TS idx = (TS)a.idx, idy = (TS)a.idy;
+    auto xm = [&](int k) { return (hside & 1) ? hx_field(a, 0, k, y) : ld(F + k * C + cxm); };
+    auto xp = [&](int k) { return (hside & 2) ? hx_field(a, 1, k, y) : ld(F + k * C + cxp); };
     TS dEx = 0, dEy = 0, dEz = 0, dBx = 0, dBy = 0, dBz = 0;
     if (a.parts & kPartAmpere) {
         // J: Ex += Jx, Ey += Re J11, Ez += -Im J11 with J11 = 2 * (f11 quadrature)
@@ -59,15 +64,15 @@ __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long c
         dEy = (TS)(2.0 * Jyr);
         dEz = (TS)(-(2.0 * Jyi));
         dEx += idy * (ld(F + 5 * C + cym) - ld(F + 5 * C + cyp));
-        dEy += -idx * (ld(F + 5 * C + cxm) - ld(F + 5 * C + cxp));
+        dEy += -idx * (xm(5) - xp(5));
         dEz += -idy * (ld(F + 3 * C + cym) - ld(F + 3 * C + cyp));
-        dEz += idx * (ld(F + 4 * C + cxm) - ld(F + 4 * C + cxp));
+        dEz += idx * (xm(4) - xp(4));
     }
     if (a.parts & kPartFaraday) {
         dBx = -idy * (ld(F + 2 * C + cym) - ld(F + 2 * C + cyp));
-        dBy = idx * (ld(F + 2 * C + cxm) - ld(F + 2 * C + cxp));
+        dBy = idx * (xm(2) - xp(2));
         dBz = idy * (ld(F + 0 * C + cym) - ld(F + 0 * C + cyp));
-        dBz += -idx * (ld(F + 1 * C + cxm) - ld(F + 1 * C + cxp));
+        dBz += -idx * (xm(1) - xp(1));
     }
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 0 * C + cell, dEx);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 1 * C + cell, dEy);
@@ -185,8 +190,15 @@ __global__ void __launch_bounds__(256) rk_stage_kernel(const StageArgs<TS> a) {
                     frp = loadf(o + 1, 0, p + 1);
                     if (m > 0) fip = loadf(o + 1, 1, p + 1);
                 }
-                const TS dxr = pv ? (load(oxm, 0) - load(oxp, 0)) * vr : TS(0);
-                const TS dxi = (m > 0 && pv) ? (load(oxm, 1) - load(oxp, 1)) * vr : TS(0);
+                // x neighbours: the halo columns at the edges of an x slab or a mirrored grid
+                auto loadx = [&](int side, int comp) -> TS {
+                    const bool edge = a.hx && (side ? cx == a.nx - 1 : cx == 0);
+                    if (!edge) return load(side ? oxp : oxm, comp);
+                    if (s == 0) return (TS)ld(hx_f00(a, side, cyy) + p);
+                    return ld(hx_plane(a, side, (long long)ld(a.plane_of + s * mstride + m) + comp, cyy) + p);
+                };
+                const TS dxr = pv ? (loadx(0, 0) - loadx(1, 0)) * vr : TS(0);
+                const TS dxi = (m > 0 && pv) ? (loadx(0, 1) - loadx(1, 1)) * vr : TS(0);
                 TS dyr = 0, dyi = 0;
                 if (has_y) {
                     dyr = pv ? (load(oym, 0) - load(oyp, 0)) * vr : TS(0);
@@ -222,7 +234,8 @@ __global__ void __launch_bounds__(256) rk_stage_kernel(const StageArgs<TS> a) {
     double Jx = 0.0, Jyr = 0.0, Jyi = 0.0;
     const int nw = (min(np, (int)blockDim.x) + 31) >> 5;
     for (int w = 0; w < nw; ++w) { Jx += sj[0][threadIdx.y][w]; Jyr += sj[1][threadIdx.y][w]; Jyi += sj[2][threadIdx.y][w]; }
-    field_update(a, cell, cxm, cxp, cym, cyp, Jx, Jyr, Jyi);
+    const int hside = a.hx ? ((cx == 0 ? 1 : 0) | (cx == a.nx - 1 ? 2 : 0)) : 0;
+    field_update(a, cell, cxm, cxp, cym, cyp, Jx, Jyr, Jyi, hside, cyy);
 }
 
 // ---------------------------------------------------------------------------

@@ -23,3 +23,4 @@ def oracle():
     yield orc
     orc.set_yadv_chain(True)
     orc.set_ee_implicit(0)
+    orc.set_mirror_x(False)
