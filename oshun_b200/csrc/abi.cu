@@ -141,20 +141,73 @@ __global__ void gather_kernel(double2* __restrict__ dst, const double* f00, cons
 // rounded to the plane type so that the stored deviation and every reader
 // (stage, collision, moments, download) use one value.
 constexpr int kProfChunks = 64;
+// A plane keeps its profile only where the cell average carries at least
+// this share of the plane's sum of squares (a large, nearly uniform
+// harmonic); elsewhere the profile is zero and its loads are skipped.
+constexpr double kProfileShare = 0.01;
 __global__ void profile_partial_kernel(const double2* __restrict__ src, const int* __restrict__ hplane,
-                                       long long cells, int np, double2* part) {
+                                       long long cells, int np, double2* part, double2* part_sq) {
     const int h = blockIdx.x, ch = blockIdx.y;
     if (hplane[h] < 0) return;   // f00 is FP64
     const long long c0 = cells * ch / kProfChunks, c1 = cells * (ch + 1) / kProfChunks;
     for (int p = threadIdx.x; p < np; p += blockDim.x) {
-        double sr = 0.0, si = 0.0;
+        double sr = 0.0, si = 0.0, qr = 0.0, qi = 0.0;
         for (long long c = c0; c < c1; ++c) {
             const double2 v = src[((long long)h * cells + c) * np + p];
             sr += v.x;
             si += v.y;
+            qr += v.x * v.x;
+            qi += v.y * v.y;
         }
         part[((long long)h * kProfChunks + ch) * np + p] = make_double2(sr, si);
+        part_sq[((long long)h * kProfChunks + ch) * np + p] = make_double2(qr, qi);
     }
+}
+// per harmonic (one CTA each): keep the profile if the cell average's sum of
+// squares is at least kProfileShare of the harmonic's, else zero it
+template <typename TS>
+__global__ void profile_keep_kernel(const double2* __restrict__ part_sq, const int* __restrict__ hplane, int nh,
+                                    long long cells, int np, double* ref64, TS* refts, int* keep) {
+    const int h = blockIdx.x;
+    const int q = hplane[h];
+    if (q < 0) return;
+    const bool cplx = hplane[nh + h] != 0;
+    __shared__ double red[2][32];
+    double mean = 0.0, tot = 0.0;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const double r = ref64[(long long)q * np + p];
+        mean += r * r;
+        double t = 0.0;
+        for (int ch = 0; ch < kProfChunks; ++ch) {
+            const double2 v = part_sq[((long long)h * kProfChunks + ch) * np + p];
+            t += v.x + (cplx ? v.y : 0.0);
+        }
+        tot += t;
+        if (cplx) {
+            const double ri = ref64[(long long)(q + 1) * np + p];
+            mean += ri * ri;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        mean += __shfl_xor_sync(0xffffffffu, mean, off);
+        tot += __shfl_xor_sync(0xffffffffu, tot, off);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = mean; red[1][threadIdx.x >> 5] = tot; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0, t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { m += red[0][w]; t += red[1][w]; }
+        red[0][0] = (m * (double)cells >= kProfileShare * t && m > 0.0) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const bool k = red[0][0] != 0.0;
+    if (threadIdx.x == 0) { keep[q] = k; if (cplx) keep[q + 1] = k; }
+    if (!k)
+        for (int p = threadIdx.x; p < np; p += blockDim.x) {
+            ref64[(long long)q * np + p] = 0.0;
+            refts[(long long)q * np + p] = TS(0);
+            if (cplx) { ref64[(long long)(q + 1) * np + p] = 0.0; refts[(long long)(q + 1) * np + p] = TS(0); }
+        }
 }
 template <typename TS>
 __global__ void profile_final_kernel(const double2* __restrict__ part, const int* __restrict__ hplane, int nh,
@@ -262,7 +315,8 @@ struct oshun_ctx {
     bool use_profile = false;
     double* d_ref64 = nullptr;
     void* d_ref_ts = nullptr;
-    double2* d_refpart = nullptr;
+    double2* d_refpart = nullptr;   // per-chunk sums, then per-chunk sums of squares
+    int* d_refkeep = nullptr;       // [nplanes]: the plane keeps a nonzero profile
     // implicit electric field (built on first use): coupling tables of
     // ImpEx, ImpEx1D, ImpEy/z and Exyz1D; J0, J(DEx), J(DEy), J(DEz), JN, DE,
     // EN ([3][cells] each) and p^3/gamma; the probe field; the zero count
@@ -389,6 +443,7 @@ StageArgs<TS> oshun_ctx::stage_args(int in_set, int out_set, int mode) const {
     std::memset(&a, 0, sizeof(a));
     a.f00_in = f00[in_set]; a.pl_in = (const TS*)pl[in_set]; a.fld_in = (const TS*)fld[in_set];
     a.pl_ref = use_profile ? (const TS*)d_ref_ts : nullptr;
+    a.pl_keep = use_profile ? d_refkeep : nullptr;
     if (xb != OSHUN_XB_PERIODIC) { a.hx = d_hx; a.hx_side = hx_side; a.hx_pl = hx_pl; a.hx_fld = hx_fld; }
     a.coef = d_coef; a.plane_of = d_plane_of;
     a.inv_pr = d_ptab; a.vr = d_ptab + cfg.nump; a.wj = d_ptab + 2 * cfg.nump;
@@ -653,6 +708,7 @@ CollideArgs collide_args(oshun_ctx* h, int do_ee, int do_l1, int do_lm, int nsub
     a.planes = h->pl[set];
     a.pl_ref = h->use_profile ? h->d_ref64 : nullptr;
     a.pl_ref32 = h->use_profile ? (const float*)h->d_ref_ts : nullptr;
+    a.pl_keep = h->use_profile ? h->d_refkeep : nullptr;
     a.planes_fp32 = h->fp32 ? 1 : 0;
     a.plane_of = h->d_plane_of; a.plane_l = h->d_plane_l; a.plane_m = h->d_plane_m;
     a.nplanes = h->nplanes;
@@ -915,7 +971,7 @@ void free_ctx(oshun_ctx* h) {
     cudaFree(h->d_hplane); cudaFree(h->d_seq); cudaFree(h->d_ptab); cudaFree(h->d_vtab); cudaFree(h->d_dense_ws);
     cudaFree(h->d_status); cudaFree(h->d_clock); cudaFree(h->d_stage); cudaFree(h->d_jw);
     cudaFree(h->d_mom_tab); cudaFree(h->d_mom);
-    cudaFree(h->d_ref64); cudaFree(h->d_ref_ts); cudaFree(h->d_refpart); cudaFree(h->d_hx);
+    cudaFree(h->d_ref64); cudaFree(h->d_ref_ts); cudaFree(h->d_refpart); cudaFree(h->d_refkeep); cudaFree(h->d_hx);
     for (int i = 0; i < 4; ++i) cudaFree(h->d_coef_imp[i]);
     cudaFree(h->d_imp); cudaFree(h->d_fe); cudaFree(h->d_zeros);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -982,7 +1038,9 @@ int oshun_create(const oshun_cfg* cfg, oshun_handle* out) {
         CKF(cudaMemset(h->d_ref64, 0, sizeof(double) * nr));
         CKF(cudaMalloc(&h->d_ref_ts, sizeof(float) * nr));
         CKF(cudaMemset(h->d_ref_ts, 0, sizeof(float) * nr));
-        CKF(cudaMalloc(&h->d_refpart, sizeof(double2) * (size_t)h->nh * kProfChunks * cfg->nump));
+        CKF(cudaMalloc(&h->d_refpart, 2 * sizeof(double2) * (size_t)h->nh * kProfChunks * cfg->nump));
+        CKF(cudaMalloc(&h->d_refkeep, sizeof(int) * (size_t)std::max(1, h->nplanes)));
+        CKF(cudaMemset(h->d_refkeep, 0, sizeof(int) * (size_t)std::max(1, h->nplanes)));
     }
     CKF(cudaMalloc(&h->d_clock, sizeof(Clock)));
     Clock ck{h->t, h->t_ee, h->t_eb};
@@ -1062,10 +1120,14 @@ int oshun_upload(oshun_handle h, const double* harmonics, const double* fields) 
     const int set = h->cur;
     const int np = h->cfg.nump;
     if (h->use_profile) {
-        profile_partial_kernel<<<dim3((unsigned)h->nh, kProfChunks), 128, 0, h->stream>>>(h->d_stage, h->d_hplane,
-                                                                                           h->cells, np, h->d_refpart);
+        double2* part_sq = h->d_refpart + (size_t)h->nh * kProfChunks * np;
+        profile_partial_kernel<<<dim3((unsigned)h->nh, kProfChunks), 128, 0, h->stream>>>(
+            h->d_stage, h->d_hplane, h->cells, np, h->d_refpart, part_sq);
         profile_final_kernel<float><<<grid_for((long long)h->nh * np, 128), 128, 0, h->stream>>>(
             h->d_refpart, h->d_hplane, h->nh, h->cells, np, h->d_ref64, (float*)h->d_ref_ts);
+        profile_keep_kernel<float><<<(unsigned)h->nh, 128, 0, h->stream>>>(part_sq, h->d_hplane, h->nh, h->cells, np,
+                                                                            h->d_ref64, (float*)h->d_ref_ts,
+                                                                            h->d_refkeep);
         CK(cudaGetLastError());
     }
     const double* ref = h->use_profile ? h->d_ref64 : nullptr;

@@ -113,7 +113,8 @@ __device__ double zlog_ei(double ne, double Te, double density_np, double Zeta) 
 // (FP64 planes hold f itself: no profile is read for them.)
 template <typename TP>
 __device__ __forceinline__ double ref_at(const CollideArgs& a, long long q, int p) {
-    if constexpr (sizeof(TP) == sizeof(float)) return a.pl_ref32 ? (double)__ldg(a.pl_ref32 + q * a.np + p) : 0.0;
+    if constexpr (sizeof(TP) == sizeof(float))
+        return (a.pl_ref32 && __ldg(a.pl_keep + q)) ? (double)__ldg(a.pl_ref32 + q * a.np + p) : 0.0;
     return 0.0;
 }
 

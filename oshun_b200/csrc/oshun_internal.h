@@ -61,6 +61,7 @@ struct StageArgs {
     // FP32 split: the l >= 1 planes store f minus this momentum profile of
     // each plane ([nplanes][np]); null: the planes store f
     const TS* pl_ref;
+    const int* pl_keep;   // [nplanes]: 0 where the plane's profile is zero (its loads are skipped)
     const double* f00_B;  const TS* pl_B;  const TS* fld_B;    // step base Y0
     double* f00_A;        TS* pl_A;        TS* fld_A;          // RK accumulator Y
     double* f00_out;      TS* pl_out;      TS* fld_out;        // next stage input (or the slope)
@@ -114,6 +115,7 @@ struct CollideArgs {
     int planes_fp32;
     const double* pl_ref; // [nplanes][np] momentum profile the planes are stored relative to (null: none)
     const float* pl_ref32;   // the same profile in FP32 (it is FP32-rounded: the values are equal)
+    const int* pl_keep;      // [nplanes]: 0 where the plane's profile is zero
     const int* plane_of;  // [(l0+1)*(m0+1)]
     const int* plane_l;   // [nplanes]: l of each plane
     const int* plane_m;   // [nplanes]: m of each plane

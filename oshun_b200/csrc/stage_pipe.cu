@@ -331,17 +331,17 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * L.slot_bytes);
-                    const TS* ref = a.pl_ref ? a.pl_ref + (long long)splane[s * mstride + m] * np : nullptr;
+                    const long long qs = splane[s * mstride + m];
+                    const TS* ref = (a.pl_ref && __ldg(a.pl_keep + qs)) ? a.pl_ref + qs * np : nullptr;
                     couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, ref, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             // the current of f = ref + stored deviation
-                            const double r0 = a.pl_ref ? (double)a.pl_ref[(long long)splane[s * mstride + m] * np + pc] : 0.0;
+                            const double r0 = ref ? (double)ref[pc] : 0.0;
                             if constexpr (m == 0) {
                                 jx += wj * ((double)sb[nb.ctr] + r0);
                             } else {
-                                const double r1 =
-                                    a.pl_ref ? (double)a.pl_ref[((long long)splane[s * mstride + m] + 1) * np + pc] : 0.0;
+                                const double r1 = ref ? (double)ref[np + pc] : 0.0;
                                 jyr += wj * ((double)sb[nb.ctr] + r0);
                                 jyi += wj * ((double)sb[seg + nb.ctr] + r1);
                             }

@@ -834,7 +834,8 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
                 acquire();
                 if (!dead) {
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * P.slot_stride + P.hdr);
-                    const TS* ref = a.pl_ref ? a.pl_ref + (long long)splane[s * mstride + m] * np : nullptr;
+                    const long long qs = splane[s * mstride + m];
+                    const TS* ref = (a.pl_ref && __ldg(a.pl_keep + qs)) ? a.pl_ref + qs * np : nullptr;
                     couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, ref, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
