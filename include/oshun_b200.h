@@ -309,21 +309,24 @@ int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile
 
 /* ---- adjoint of the small step ------------------------------------------- */
 
-/* No counterpart in the reference, which computes no derivatives.  For 1D
- * runs with m0 = 0 (numy = 1, tridiagonal collisions, nump <= 256), FP64 or
- * the FP32 bulk form (precision OSHUN_FP32_SPLIT: the forward steps keep the
- * l >= 1 planes and fields in FP32, and the stage transposes run in FP32
- * arithmetic; f00, the collision transposes and the cotangent vectors stay
- * FP64; the flag OSHUN_FLAG_IMPLICIT_EE is refused):
- * the vector-Jacobian product of one small step (oshun_step's sequence:
- * RK4 Vlasov-Maxwell step, then, with `collisions`, the e-e substeps and the
- * implicit f_l solves).  State vectors are device arrays of
+/* No counterpart in the reference, which computes no derivatives.  For any
+ * grid (1D or 2D, any m0) with tridiagonal collisions and nump <= 256, in
+ * FP64; for 1D runs with m0 = 0 also the FP32 bulk form (precision
+ * OSHUN_FP32_SPLIT: the forward steps keep the l >= 1 planes and fields in
+ * FP32, and the stage transposes run in FP32 arithmetic; f00, the collision
+ * transposes and the cotangent vectors stay FP64).  The flag
+ * OSHUN_FLAG_IMPLICIT_EE is refused.  The entry points give the
+ * vector-Jacobian product of one small step (oshun_step's sequence: RK4
+ * Vlasov-Maxwell step, then, with `collisions`, the e-e substeps and the
+ * implicit f_lm solves).  State vectors are device arrays of
  * oshun_adjoint_state_size doubles in the plane layout: the f00 plane, the
- * l >= 1 planes (f[l][x][p]), the 6 field planes.  (t, t_ee, t_eb) are the
+ * l >= 1 planes (oshun_plane_index; [numy][numx][nump] each), the 6 field
+ * planes.  (t, t_ee, t_eb) are the
  * RK, e-e and implicit clocks before the step (Runge_Kutta_4::t,
  * Explicit_EC_FP::t, Euler_Backward::t): they fix the step's e-e substeps
- * and implicit step as in the forward.  Cotangents of the fields other than
- * E_x come back zero: with m0 = 0 they never act on f or E_x. */
+ * and implicit step as in the forward.  For 1D runs with m0 = 0 the
+ * cotangents of the fields other than E_x come back zero: they never act on
+ * f or E_x there. */
 typedef struct oshun_adj_ctx* oshun_adjoint;
 int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out);
 int oshun_adjoint_destroy(oshun_adjoint a);
@@ -362,7 +365,9 @@ int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, 
  * With either, it also checks the result planes for NaN/Inf, waits for the
  * stream, stores the outputs and returns OSHUN_ERR_NUMERIC when bit 1 is set.
  * The first call on a device looks up the array's device address; make it
- * before any stream capture.  Every call shares the array and it keeps the
+ * before any stream capture.  Later calls can be captured with nondominant
+ * and flags NULL (their read-back is refused, OSHUN_ERR_UNSUPPORTED, while
+ * the stream captures).  Every call shares the array and it keeps the
  * last call's contents: calls that overlap on the GPU race on it. */
 int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, double* planes, double Dt, void* stream,
                               long long* nondominant, int* flags);

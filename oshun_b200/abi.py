@@ -237,6 +237,12 @@ class Handle:
         """nsteps of the implicit-E small step (mask bits as oshun_rk2_imp_step)."""
         self._check(self.lib.oshun_rk2_imp_step(self._h, nsteps, mask), "oshun_rk2_imp_step")
 
+    def plane_index(self, l: int, m: int) -> int:
+        """Plane of Re f_lm (l >= 1; Im follows), -1 for f00."""
+        q = ctypes.c_int()
+        self._check(self.lib.oshun_plane_index(self._h, l, m, ctypes.byref(q)), "oshun_plane_index")
+        return q.value
+
     def set_x_boundary(self, mode: int) -> None:
         """OSHUN_XB_PERIODIC, OSHUN_XB_MIRROR or OSHUN_XB_HALO (an x slab)."""
         self._check(self.lib.oshun_set_x_boundary(self._h, int(mode)), "oshun_set_x_boundary")

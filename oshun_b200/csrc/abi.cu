@@ -27,6 +27,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint2d.cuh"
 #include "oshun_internal.h"
 
 namespace oshun {
@@ -2240,6 +2241,7 @@ struct oshun_adj_ctx {
     double *s2 = nullptr, *s3 = nullptr, *s4 = nullptr, *y1 = nullptr;
     double *lam1 = nullptr, *c = nullptr, *a = nullptr, *acc = nullptr;
     adj::Coef1* d_coef1 = nullptr;
+    bool general = false;            // a 2D grid or m0 > 0: the general stage transpose
     double* ws = nullptr;
     long long ws_cap = 0;            // doubles
 };
@@ -2295,6 +2297,18 @@ adj::Grid1 adj_grid(const oshun_adj_ctx* a) {
     return g;
 }
 
+adj2::Grid2 adj_grid2(const oshun_ctx* h) {
+    adj2::Grid2 g;
+    g.np = h->cfg.nump; g.nx = h->cfg.numx; g.ny = h->cfg.numy; g.l0 = h->cfg.l0; g.m0 = h->cfg.m0;
+    g.nplanes = h->nplanes;
+    g.cells = h->cells; g.pstride = h->pstride;
+    g.invp = h->d_ptab; g.vr = h->d_ptab + h->cfg.nump; g.wj = h->d_ptab + 2 * h->cfg.nump;
+    g.coef = h->d_coef; g.plane_of = h->d_plane_of;
+    g.g00_s = h->g00_s; g.g00_inv = h->g00_inv; g.g00_gr = h->g00_gr;
+    g.idx = h->idx; g.idy = h->idy;
+    return g;
+}
+
 adj::CollTables adj_tables(const oshun_ctx* h) {
     adj::CollTables T;
     const int np = h->cfg.nump;
@@ -2314,8 +2328,13 @@ extern "C" {
 int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out) {
     if (!out || !cfg) { set_error("NULL argument"); return OSHUN_ERR_ARG; }
     *out = nullptr;
-    if (cfg->numy != 1 || cfg->m0 != 0 || !cfg->if_tridiagonal || ((cfg->nump + 31) / 32) * 32 > 256) {
-        set_error("the adjoint covers 1D runs (numy = 1) with m0 = 0, tridiagonal collisions, nump <= 256");
+    if (!cfg->if_tridiagonal || ((cfg->nump + 31) / 32) * 32 > 256) {
+        set_error("the adjoint covers tridiagonal collisions and nump <= 256");
+        return OSHUN_ERR_UNSUPPORTED;
+    }
+    const bool general = cfg->numy > 1 || cfg->m0 > 0;
+    if (general && cfg->precision != OSHUN_FP64) {
+        set_error("the FP32 bulk adjoint covers 1D runs with m0 = 0");
         return OSHUN_ERR_UNSUPPORTED;
     }
     if (cfg->flags & OSHUN_FLAG_IMPLICIT_EE) {
@@ -2333,6 +2352,11 @@ int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out) {
     double** bufs[] = {&a->s2, &a->s3, &a->s4, &a->y1, &a->lam1, &a->c, &a->a, &a->acc};
     for (double** b : bufs)
         if (cudaMalloc(b, sizeof(double) * a->n) != cudaSuccess) { set_error("cudaMalloc failed"); return fail(OSHUN_ERR_CUDA); }
+    a->general = general;
+    if (general) {
+        *out = a;
+        return OSHUN_OK;
+    }
     const int l0 = cfg->l0;
     std::vector<double> cf((size_t)(l0 + 1) * 16);
     std::vector<adj::Coef1> c1(l0 + 1);
@@ -2409,18 +2433,20 @@ int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, 
         const double hsub = (t_new - t_ee) / (double)nsub;
         const double Dt = t_new - t_eb;
         const long long wsz = adj::coll_ws(h->cfg.nump, h->cfg.l0, nsub);
-        if (wsz * h->cfg.numx > a->ws_cap) {
+        if (wsz * h->cells > a->ws_cap) {
             CK(cudaStreamSynchronize(h->stream));
             cudaFree(a->ws);
             a->ws = nullptr;
-            CK(cudaMalloc(&a->ws, sizeof(double) * wsz * h->cfg.numx));
-            a->ws_cap = wsz * h->cfg.numx;
+            CK(cudaMalloc(&a->ws, sizeof(double) * wsz * h->cells));
+            a->ws_cap = wsz * h->cells;
         }
-        CK(launch_collide_adj(adj_tables(h), h->cfg.l0, h->cfg.numx, a->y1, a->lam1, 1, 1, nsub, hsub, Dt, a->ws, wsz,
-                              h->stream));
+        const int mmax = h->cfg.if_implicit1D ? 0 : h->cfg.m0;
+        CK(launch_collide_adj(adj_tables(h), h->cfg.l0, (int)h->cells, a->y1, a->lam1, 1, 1, nsub, hsub, Dt, a->ws,
+                              wsz, h->stream, a->general ? h->d_plane_of : nullptr, h->cfg.m0, mmax));
     }
     // RK4 transpose
     const adj::Grid1 g = adj_grid(a);
+    const adj2::Grid2 g2 = adj_grid2(h);
     const long long n = a->n;
     CK(cudaMemcpyAsync(a->acc, a->lam1, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     const double* S[4] = {y, a->s2, a->s3, a->s4};
@@ -2429,7 +2455,8 @@ int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, 
     for (int st = 3; st >= 0; --st) {
         if (st == 3) CK(launch_rk_combine(a->c, a->lam1, w_out[3], a->lam1, 0.0, nullptr, 0.0, n, h->stream));
         else CK(launch_rk_combine(a->c, a->lam1, w_out[st], a->a, w_in[st + 1], nullptr, 0.0, n, h->stream));
-        CK(launch_stage_vjp(g, S[st], a->c, a->a, h->stream, h->fp32));
+        if (a->general) CK(launch_stage_vjp2(g2, S[st], a->c, a->a, h->stream));
+        else CK(launch_stage_vjp(g, S[st], a->c, a->a, h->stream, h->fp32));
         CK(launch_rk_combine(a->acc, a->acc, 1.0, a->a, 1.0, nullptr, 0.0, n, h->stream));
     }
     CK(cudaMemcpyAsync(lam, a->acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));

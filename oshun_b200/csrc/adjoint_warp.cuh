@@ -346,11 +346,21 @@ __device__ void thomas_T(const double* a, const double* tb, const double* c, con
 // post-e-e f00 and 27 np of scratch
 __host__ __device__ inline long long coll_ws(int np, int nsub) { return (long long)np * (nsub + 1 + 27); }
 
+// the collided planes of a cell: for each l >= 1 the planes of m <= min(l,
+// mmax) (Re, and Im for m > 0), all sharing the l matrix; plane q of the
+// cell is at base + q * stride
+struct CellPlanes {
+    const int* plane_of;   // [(l0+1)(m0+1)]: plane of Re f_lm
+    int m0, mmax;
+};
+
 // adj::collide_cell_T on one warp: lam00 / laml hold the cotangents of the
-// outputs and receive those of the inputs
+// outputs and receive those of the inputs.  Without `P` (plane_of null) the
+// planes are f_l, l = 1..l0, lstride apart (m0 = 0); with it, every
+// collided plane of each l (lstride, lamstride: the plane strides)
 __device__ void collide_cell_T(const CollTables& T, int l0, const double* f00_in, const double* fl_in,
                                long long lstride, int ee, int eb, int nsub, double hsub, double Dt, double* lam00,
-                               double* laml, long long lamstride, double* w) {
+                               double* laml, long long lamstride, double* w, const CellPlanes P = {nullptr, 0, 0}) {
     const int n = T.np;
     const int lane = lane_id();
     double* fstart = w;
@@ -373,19 +383,25 @@ __device__ void collide_cell_T(const CollTables& T, int l0, const double* f00_in
         __syncwarp();
         for (int l = 1; l <= l0; ++l) {
             const double ll1 = l * ((-0.5) * (l + 1.0));
-            thomas(ta, tb, tc, sc, l, n, fl_in + (long long)(l - 1) * lstride, x, tw);
-            double* lam = laml + (long long)(l - 1) * lamstride;
-            thomas_T(ta, tb, tc, sc, l, n, lam, y, tw);
-            for (int i = lane; i < n; i += 32) {
-                if (i >= 1) la[i] += -y[i] * x[i - 1];
-                if (i + 1 < n) lc[i] += -y[i] * x[i + 1];
-                const double lbi = -y[i] * x[i];
-                if (!(i == 0 && l > 1)) lb[i] += lbi;
-                ls[i] += -ll1 * lbi;
-            }
-            __syncwarp();
-            for (int i = lane; i < n; i += 32) lam[i] = y[i];
-            __syncwarp();
+            const int mtop = P.plane_of ? (l < P.mmax ? l : P.mmax) : 0;
+            for (int m = 0; m <= mtop; ++m)
+                for (int comp = 0; comp < (m > 0 ? 2 : 1); ++comp) {
+                    const long long q =
+                        P.plane_of ? (long long)P.plane_of[l * (P.m0 + 1) + m] + comp : (long long)(l - 1);
+                    thomas(ta, tb, tc, sc, l, n, fl_in + q * lstride, x, tw);
+                    double* lam = laml + q * lamstride;
+                    thomas_T(ta, tb, tc, sc, l, n, lam, y, tw);
+                    for (int i = lane; i < n; i += 32) {
+                        if (i >= 1) la[i] += -y[i] * x[i - 1];
+                        if (i + 1 < n) lc[i] += -y[i] * x[i + 1];
+                        const double lbi = -y[i] * x[i];
+                        if (!(i == 0 && l > 1)) lb[i] += lbi;
+                        ls[i] += -ll1 * lbi;
+                    }
+                    __syncwarp();
+                    for (int i = lane; i < n; i += 32) lam[i] = y[i];
+                    __syncwarp();
+                }
         }
         adjw::reset_coeff_T(T, g, Dt, la, lb, lc, ls, lam00, tw);
     }

@@ -228,7 +228,14 @@ extern "C" int oshun_collide_flm_noalloc(const oshun_cfg* cfg, double* f00, doub
     CKN(launch_collide(a, st, smem, blocks));
     if (nondominant || flags) {
         // NaN/Inf in the result planes sets bit 1; then wait for the stream
-        // and report the status word
+        // and report the status word (a read-back that a stream capture
+        // cannot hold: refused while the stream is capturing)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CKN(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone) {
+            set_error("noalloc collision step: nondominant/flags read back the status; pass NULL while capturing");
+            return OSHUN_ERR_UNSUPPORTED;
+        }
         CKN(launch_nan_check(f00, planes, 0, cells * np, (long long)nplanes * cells * np, nullptr, 0, dstatus, st));
         int h_status[2] = {0, 0};
         CKN(cudaMemcpyAsync(h_status, dstatus, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));

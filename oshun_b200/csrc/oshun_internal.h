@@ -215,7 +215,8 @@ cudaError_t launch_stage_vjp(const adj::Grid1& g, const double* s, const double*
 cudaError_t launch_convert(const double* src, float* dst, long long n, cudaStream_t st);
 cudaError_t launch_convert(const float* src, double* dst, long long n, cudaStream_t st);
 cudaError_t launch_collide_adj(const adj::CollTables& T, int l0, int nx, const double* y, double* lam, int ee, int eb,
-                               int nsub, double hsub, double Dt, double* ws, long long wsz, cudaStream_t st);
+                               int nsub, double hsub, double Dt, double* ws, long long wsz, cudaStream_t st,
+                               const int* plane_of = nullptr, int m0 = 0, int mmax = 0);
 cudaError_t launch_rk_combine(double* out, const double* v0, double a0, const double* v1, double a1, const double* v2,
                               double a2, long long n, cudaStream_t st);
 // tridiagonal collision step of a batch whose problems share E = ceil(np/32) <= 8
