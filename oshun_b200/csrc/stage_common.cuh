@@ -7,15 +7,26 @@
 
 namespace oshun {
 
+// Roundings spelled out: the RK updates and the field updates run in several
+// kernels (single-problem, batched, global-load), and a product the compiler
+// fused into an add in one and not in another would make their results
+// differ in the last bit
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // out/B/A are base pointers (out may be null: stage 4 has no next input)
 template <typename TS>
 __device__ __forceinline__ void rk_update(int mode, int first, double c1, double c2, TS* out, const TS* B, TS* A,
                                           long long i, TS k) {
     if (mode == 1) { out[i] = k; return; }
-    const TS t = k * (TS)c1;
+    const TS t = mul_rn(k, (TS)c1);
     const TS b = B[i];
-    if (out) out[i] = b + t;
-    A[i] = (first ? b : A[i]) + t * (TS)c2;
+    if (out) out[i] = add_rn(b, t);
+    A[i] = fma_rn(t, (TS)c2, first ? b : A[i]);
 }
 
 // Couplings of source (s, m) at one momentum point.  fr/fi: value, frm/frp

@@ -289,11 +289,11 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                     if (a.mode == 1) {
                         a.f00_out[o] = k;
                     } else {
-                        const double tt = k * a.c1;
+                        const double tt = mul_rn(k, a.c1);
                         const double b = reinterpret_cast<const double*>(base)[roff];
-                        if (a.f00_out) a.f00_out[o] = b + tt;
-                        a.f00_A[o] = (a.first ? b : reinterpret_cast<const double*>(base + L.row_arr_bytes)[roff]) +
-                                     tt * a.c2;
+                        if (a.f00_out) a.f00_out[o] = add_rn(b, tt);
+                        a.f00_A[o] = fma_rn(tt, a.c2,
+                                            a.first ? b : reinterpret_cast<const double*>(base + L.row_arr_bytes)[roff]);
                     }
                 } else {
                     const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);

@@ -413,17 +413,13 @@ __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long c
     const TS idx = (TS)a.idx, idy = (TS)a.idy;
     auto xm = [&](int k) { return (hside & 1) ? hx_field(a, 0, k, y) : ldg(F + k * C + cxm); };
     auto xp = [&](int k) { return (hside & 2) ? hx_field(a, 1, k, y) : ldg(F + k * C + cxp); };
-    TS dEx = (TS)Jx;
-    TS dEy = (TS)(2.0 * Jyr);
-    TS dEz = (TS)(-(2.0 * Jyi));
-    dEx += idy * (ldg(F + 5 * C + cym) - ldg(F + 5 * C + cyp));
-    dEy += -idx * (xm(5) - xp(5));
-    dEz += -idy * (ldg(F + 3 * C + cym) - ldg(F + 3 * C + cyp));
-    dEz += idx * (xm(4) - xp(4));
-    TS dBx = -idy * (ldg(F + 2 * C + cym) - ldg(F + 2 * C + cyp));
-    TS dBy = idx * (xm(2) - xp(2));
-    TS dBz = idy * (ldg(F + 0 * C + cym) - ldg(F + 0 * C + cyp));
-    dBz += -idx * (xm(1) - xp(1));
+    const TS dEx = fma_rn(idy, ldg(F + 5 * C + cym) - ldg(F + 5 * C + cyp), (TS)Jx);
+    const TS dEy = fma_rn(-idx, xm(5) - xp(5), (TS)(2.0 * Jyr));
+    const TS dEz = fma_rn(idx, xm(4) - xp(4),
+                          fma_rn(-idy, ldg(F + 3 * C + cym) - ldg(F + 3 * C + cyp), (TS)(-(2.0 * Jyi))));
+    const TS dBx = mul_rn(-idy, ldg(F + 2 * C + cym) - ldg(F + 2 * C + cyp));
+    const TS dBy = mul_rn(idx, xm(2) - xp(2));
+    const TS dBz = fma_rn(-idx, xm(1) - xp(1), mul_rn(idy, ldg(F + 0 * C + cym) - ldg(F + 0 * C + cyp)));
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 0 * C + cell, dEx);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 1 * C + cell, dEy);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 2 * C + cell, dEz);
@@ -491,10 +487,10 @@ __device__ __forceinline__ void store_row(const StageArgs<TS>& a, const int mtop
 #pragma unroll
         for (int comp = 0; comp < (m > 0 ? 2 : 1); ++comp) {
             const int k = kk + comp;
-            const TS t = k_of(m, comp) * c1;
+            const TS t = mul_rn(k_of(m, comp), c1);
             const TS b = Bs[k * rstride];
-            if (has_out) out[k * ps] = b + t;
-            A[k * ps] = (first ? b : As[k * rstride]) + t * c2;
+            if (has_out) out[k * ps] = add_rn(b, t);
+            A[k * ps] = fma_rn(t, c2, first ? b : As[k * rstride]);
         }
     });
 }
@@ -795,11 +791,11 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
                     if (a.mode == 1) {
                         a.f00_out[o] = k;
                     } else {
-                        const double tt = k * a.c1;
+                        const double tt = mul_rn(k, a.c1);
                         const double b = reinterpret_cast<const double*>(base)[roff];
-                        if (a.f00_out) a.f00_out[o] = b + tt;
-                        a.f00_A[o] = (a.first ? b : reinterpret_cast<const double*>(base + P.row_arr_bytes)[roff]) +
-                                     tt * a.c2;
+                        if (a.f00_out) a.f00_out[o] = add_rn(b, tt);
+                        a.f00_A[o] = fma_rn(tt, a.c2,
+                                            a.first ? b : reinterpret_cast<const double*>(base + P.row_arr_bytes)[roff]);
                     }
                 } else {
                     const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);

@@ -60,19 +60,14 @@ __device__ __forceinline__ void field_update(const StageArgs<TS>& a, long long c
     TS dEx = 0, dEy = 0, dEz = 0, dBx = 0, dBy = 0, dBz = 0;
     if (a.parts & kPartAmpere) {
         // J: Ex += Jx, Ey += Re J11, Ez += -Im J11 with J11 = 2 * (f11 quadrature)
-        dEx = (TS)Jx;
-        dEy = (TS)(2.0 * Jyr);
-        dEz = (TS)(-(2.0 * Jyi));
-        dEx += idy * (ld(F + 5 * C + cym) - ld(F + 5 * C + cyp));
-        dEy += -idx * (xm(5) - xp(5));
-        dEz += -idy * (ld(F + 3 * C + cym) - ld(F + 3 * C + cyp));
-        dEz += idx * (xm(4) - xp(4));
+        dEx = fma_rn(idy, ld(F + 5 * C + cym) - ld(F + 5 * C + cyp), (TS)Jx);
+        dEy = fma_rn(-idx, xm(5) - xp(5), (TS)(2.0 * Jyr));
+        dEz = fma_rn(idx, xm(4) - xp(4), fma_rn(-idy, ld(F + 3 * C + cym) - ld(F + 3 * C + cyp), (TS)(-(2.0 * Jyi))));
     }
     if (a.parts & kPartFaraday) {
-        dBx = -idy * (ld(F + 2 * C + cym) - ld(F + 2 * C + cyp));
-        dBy = idx * (xm(2) - xp(2));
-        dBz = idy * (ld(F + 0 * C + cym) - ld(F + 0 * C + cyp));
-        dBz += -idx * (xm(1) - xp(1));
+        dBx = mul_rn(-idy, ld(F + 2 * C + cym) - ld(F + 2 * C + cyp));
+        dBy = mul_rn(idx, xm(2) - xp(2));
+        dBz = fma_rn(-idx, xm(1) - xp(1), mul_rn(idy, ld(F + 0 * C + cym) - ld(F + 0 * C + cyp)));
     }
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 0 * C + cell, dEx);
     rk_update(a.mode, a.first, a.c1, a.c2, a.fld_out, a.fld_B, a.fld_A, 1 * C + cell, dEy);
