@@ -111,6 +111,13 @@ __device__ double zlog_ei(double ne, double Te, double density_np, double Zeta) 
 // The planes hold f - ref when a momentum profile is given (FP32 split):
 // f of plane q at momentum point p, and the stored value of f.
 // (FP64 planes hold f itself: no profile is read for them.)
+// The profile row of plane q when the plane keeps one (FP32 planes), else null:
+// looked up once per plane, so the plane loops branch once per plane
+template <typename TP>
+__device__ __forceinline__ const float* ref_row(const CollideArgs& a, long long q) {
+    if constexpr (sizeof(TP) == sizeof(float)) return (a.pl_ref32 && __ldg(a.pl_keep + q)) ? a.pl_ref32 + q * a.np : nullptr;
+    return nullptr;
+}
 template <typename TP>
 __device__ __forceinline__ double ref_at(const CollideArgs& a, long long q, int p) {
     if constexpr (sizeof(TP) == sizeof(float))
@@ -847,9 +854,15 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
 #pragma unroll
         for (int b = 0; b < P; ++b) {
             const TP* g = planes + (q0 + b) * a.pstride + cell * n;
+            const float* rp = (j + b < nq) ? ref_row<TP>(a, q0 + b) : nullptr;
+            if (rp) {
 #pragma unroll
-            for (int e = 0; e < E; ++e)
-                r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] + ref_at<TP>(a, q0 + b, i0 + e) : 0.0;
+                for (int e = 0; e < E; ++e)
+                    r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] + (double)__ldg(rp + i0 + e) : 0.0;
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] : 0.0;
+            }
         }
     };
 
@@ -983,12 +996,13 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
             for (int b = 0; b < P; ++b) {
                 double x = __shfl_down_sync(kFull, Bb[b], 1);
                 TP* g = planes + (q0 + b) * a.pstride + cell * n;
+                const float* rp = (j + b < nq) ? ref_row<TP>(a, q0 + b) : nullptr;
 #pragma unroll
                 for (int e = E - 1; e >= 0; --e) {
                     const int i = i0 + e;
                     if (i < n) {
                         x = (i == n - 1) ? cur[b][e] : cur[b][e] - cp[e] * x;
-                        if (j + b < nq) g[i] = (TP)(x - ref_at<TP>(a, q0 + b, i));
+                        if (j + b < nq) g[i] = (TP)(rp ? x - (double)__ldg(rp + i) : x);
                     }
                 }
             }
