@@ -260,12 +260,22 @@ __device__ __forceinline__ void couple_src3_ri(TS (&R0)[MC + 1], TS (&R1)[MC + 1
         // Em G -> (s+1, M+1), Em H -> (s-1, M+1), y advection, (Bz + iBy)/2 f -> (s, M+1)
         const TS gy = c.em_g * th.eyg, gz = c.em_g * th.ezg;
         const TS hy = c.em_h * th.ey, hz = c.em_h * th.ez;
-        R2[M + 1] += gy * Gr + gz * Gi + c.ay_pp * dyr;
-        I2[M + 1] += gy * Gi - gz * Gr + c.ay_pp * dyi;
-        R0[M + 1] += hy * Hr + hz * Hi + c.ay_mp * dyr;
-        I0[M + 1] += hy * Hi - hz * Hr + c.ay_mp * dyi;
-        R1[M + 1] += th.hbz * fr - th.hby * fi;
-        I1[M + 1] += th.hbz * fi + th.hby * fr;
+        if constexpr (DN) {
+            R2[M + 1] += gy * Gr + gz * Gi + c.ay_pp * dyr;
+            I2[M + 1] += gy * Gi - gz * Gr + c.ay_pp * dyi;
+            R0[M + 1] += hy * Hr + hz * Hi + c.ay_mp * dyr;
+            I0[M + 1] += hy * Hi - hz * Hr + c.ay_mp * dyi;
+            R1[M + 1] += th.hbz * fr - th.hby * fi;
+            I1[M + 1] += th.hbz * fi + th.hby * fr;
+        } else {
+            // an m = 0 source is real: its imaginary terms are zero
+            R2[M + 1] += gy * Gr + c.ay_pp * dyr;
+            I2[M + 1] -= gz * Gr;
+            R0[M + 1] += hy * Hr + c.ay_mp * dyr;
+            I0[M + 1] -= hz * Hr;
+            R1[M + 1] += th.hbz * fr;
+            I1[M + 1] += th.hby * fr;
+        }
     }
     if constexpr (DN) {
         // Ep H -> (s-1, M-1), Ep G -> (s+1, M-1), y advection, -i M Bx f -> (s, M),
