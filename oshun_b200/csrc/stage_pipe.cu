@@ -24,11 +24,14 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
     uint64_t* empty = full + kMaxDepth;
     uint64_t* rowfull = empty + kMaxDepth;
     uint64_t* rowempty = rowfull + 2;
+    uint64_t* f0full = rowempty + 2;
+    uint64_t* f0empty = f0full + 1;
     CoefT<TS>* scoef = reinterpret_cast<CoefT<TS>*>(smem + L.off_coef);
     int* splane = reinterpret_cast<int*>(smem + L.off_plane);
-    TS* sfld = reinterpret_cast<TS*>(smem + L.off_fld);      // [2 tiles][6][tx]: the tile's E and B
+    unsigned char* sfld = smem + L.off_fld;    // [2 tiles][6]: the spans holding the tile's E and B
     unsigned char* slots = smem + L.off_slots;
-    unsigned char* rows = smem + L.off_rows;
+    unsigned char* rows = smem + L.off_rows;          // rows l >= 1: [2 buffers][B, A]
+    unsigned char* f0row = smem + L.off_f00;          // the f00 row: [B, A]
     const bool need_B = a.mode != 1;
     const bool need_A = a.mode != 1 && !a.first;
     // Y0 enters the update only through the stage output and the first
@@ -51,6 +54,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         if (tid == 0) {
             for (int k = 0; k < D; ++k) { mbar_init(full + k, 1); mbar_init(empty + k, ncw); }
             for (int k = 0; k < 2; ++k) { mbar_init(rowfull + k, 1); mbar_init(rowempty + k, ncw); }
+            mbar_init(f0full, 1);
+            mbar_init(f0empty, ncw);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
     }
@@ -137,50 +142,70 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                     mbar_wait(full + (idx % D), (uint32_t)((idx / D) & 1), wlim);
             }
         } else if (tid == nct + 32 && need_B) {
-            // row warp: Y0 (and Y) of each target row, up to two rows ahead of its epilogue
-            int issued = 0;
+            // row warp, per tile: the f00 row (Y0 and Y) with the tile's fields
+            // into the f00 buffer, a tile ahead of its use; then Y0 (and Y) of
+            // each target row l >= 1, up to two rows ahead of its epilogue
+            int issued = 0;      // rows l >= 1
+            int f0_issued = 0;   // f00 rows (one per tile)
             bool ok = true;
-            int ti = 0;
-            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++ti) {
+            const uint32_t nb = (need_Y0 ? 1 : 0) + (need_A ? 1 : 0);
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 const int y = tile / tiles_x;
                 const int x0 = (tile - y * tiles_x) * tx;
                 const int txv = min(tx, nx - x0);
                 const long long base_cell = (long long)y * nx + x0;
-                for (int t = 0; t <= a.l0; ++t) {
+                // the buffer is free once every consumer warp has stored the
+                // previous tile's row 0 (and so has read that tile's fields)
+                if (f0_issued >= 1 && !mbar_wait(f0empty, (uint32_t)((f0_issued - 1) & 1), wlim)) {
+                    ok = false;
+                    break;
+                }
+                {
+                    // the tile's fields: per field one bulk copy of the 16-byte
+                    // aligned span holding its txv values (a span never leaves the
+                    // allocation's pages); then Y0 and Y of the f00 row
+                    unsigned char* fd = sfld + (size_t)(f0_issued & 1) * 6 * L.fld_stride;
+                    const unsigned char* fsrc[6];
+                    uint32_t fsz[6], ftot = 0;
+#pragma unroll
+                    for (int f = 0; f < 6; ++f) {
+                        const uintptr_t lo = reinterpret_cast<uintptr_t>(a.fld_in + f * a.cells + base_cell);
+                        const uintptr_t hi = lo + (uintptr_t)txv * sizeof(TS);
+                        fsrc[f] = reinterpret_cast<const unsigned char*>(lo & ~(uintptr_t)15);
+                        fsz[f] = (uint32_t)(((hi + 15) & ~(uintptr_t)15) - (lo & ~(uintptr_t)15));
+                        ftot += fsz[f];
+                    }
+                    const uint32_t b = (uint32_t)txv * np * 8;
+                    mbar_expect_tx(f0full, nb * b + ftot);
+#pragma unroll
+                    for (int f = 0; f < 6; ++f) bulk_g2s(fd + (size_t)f * L.fld_stride, fsrc[f], fsz[f], f0full);
+                    if (need_Y0) bulk_g2s(f0row, a.f00_B + base_cell * np, b, f0full);
+                    if (need_A) bulk_g2s(f0row + L.f00_arr_bytes, a.f00_A + base_cell * np, b, f0full);
+                    ++f0_issued;
+                }
+                for (int t = 1; t <= a.l0; ++t) {
                     const int rb = issued & 1, k = issued >> 1;
                     if (k >= 1 && !mbar_wait(rowempty + rb, (uint32_t)((k - 1) & 1), wlim)) { ok = false; break; }
-                    unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
-                    const uint32_t nb = (need_Y0 ? 1 : 0) + (need_A ? 1 : 0);
-                    if (t == 0) {
-                        // the tile's fields travel with row 0: stored before the
-                        // arrive below, whose release orders them for the consumers;
-                        // the buffer of tile ti - 2 was read at that tile's start
-                        TS* fd = sfld + (size_t)(ti & 1) * 6 * tx;
-                        for (int f = 0; f < 6; ++f)
-                            for (int cc = 0; cc < txv; ++cc) fd[f * tx + cc] = ldg(a.fld_in + f * a.cells + base_cell + cc);
-                        const uint32_t b = (uint32_t)txv * np * 8;
-                        mbar_expect_tx(rowfull + rb, nb * b);
-                        if (need_Y0) bulk_g2s(base, a.f00_B + base_cell * np, b, rowfull + rb);
-                        if (need_A) bulk_g2s(base + L.row_arr_bytes, a.f00_A + base_cell * np, b, rowfull + rb);
-                    } else {
-                        const int np_row = 1 + 2 * min(t, a.m0);
-                        const uint32_t b = (uint32_t)txv * np * sizeof(TS);
-                        mbar_expect_tx(rowfull + rb, nb * np_row * b);
-                        const long long q0 = splane[t * mstride];
-                        for (int kk = 0; kk < np_row; ++kk) {
-                            const long long off = (q0 + kk) * a.pstride + base_cell * np;
-                            const size_t d = (size_t)kk * tx * np * sizeof(TS);
-                            if (need_Y0) bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
-                            if (need_A) bulk_g2s(base + L.row_arr_bytes + d, a.pl_A + off, b, rowfull + rb);
-                        }
+                    unsigned char* base = rows + (size_t)rb * 2 * L.rowl_arr_bytes;
+                    const int np_row = 1 + 2 * min(t, a.m0);
+                    const uint32_t b = (uint32_t)txv * np * sizeof(TS);
+                    mbar_expect_tx(rowfull + rb, nb * np_row * b);
+                    const long long q0 = splane[t * mstride];
+                    for (int kk = 0; kk < np_row; ++kk) {
+                        const long long off = (q0 + kk) * a.pstride + base_cell * np;
+                        const size_t d = (size_t)kk * tx * np * sizeof(TS);
+                        if (need_Y0) bulk_g2s(base + d, a.pl_B + off, b, rowfull + rb);
+                        if (need_A) bulk_g2s(base + L.rowl_arr_bytes + d, a.pl_A + off, b, rowfull + rb);
                     }
                     ++issued;
                 }
             }
             if (!ok) {
                 atomicOr(a.err, 16);
+                // bounded drain of the copies that may still be in flight
                 for (int t = max(0, issued - 2); t < issued; ++t)
                     mbar_wait(rowfull + (t & 1), (uint32_t)((t >> 1) & 1), wlim);
+                if (f0_issued >= 1) mbar_wait(f0full, (uint32_t)((f0_issued - 1) & 1), wlim);
             }
         }
         return;
@@ -241,15 +266,20 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
 
         Th<TS> th;
         if (need_B) {
-            // the row warp staged this tile's fields with its row 0
-            const int rb = rows_used & 1;
-            if (!dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1), wlim)) {
+            // the row warp staged this tile's fields with its f00 row
+            if (!dead && !mbar_wait(f0full, (uint32_t)(tile_iter & 1), wlim)) {
                 atomicOr(a.err, 16);
                 dead = true;
             }
-            const TS* fd = sfld + (size_t)(tile_iter & 1) * 6 * tx + cc;
-            th.ex = fd[0]; th.ey = fd[tx]; th.ez = fd[2 * tx];
-            th.bx = fd[3 * tx]; th.by = fd[4 * tx]; th.bz = fd[5 * tx];
+            // field f of this cell: its span's start is the aligned-down address
+            const unsigned char* fb = sfld + (size_t)(tile_iter & 1) * 6 * L.fld_stride;
+            const long long c0 = (long long)y * nx + x0;
+            auto fval = [&](int f) -> TS {
+                const uintptr_t addr = reinterpret_cast<uintptr_t>(a.fld_in + f * a.cells + c0);
+                return reinterpret_cast<const TS*>(fb + (size_t)f * L.fld_stride + (addr & 15))[cc];
+            };
+            th.ex = fval(0); th.ey = fval(1); th.ez = fval(2);
+            th.bx = fval(3); th.by = fval(4); th.bz = fval(5);
         } else {
             th.ex = ldg(a.fld_in + cell);
             th.ey = ldg(a.fld_in + a.cells + cell);
@@ -277,40 +307,43 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
 
         // RK epilogue of target row t (slopes Rt, It) from the staged Y0/Y rows
         auto epilogue = [&](const int t, const Acc<TS, MC>& At) {
+            if (t == 0) {
+                // the f00 buffer: its wait was the tile's first
+                if (!dead && pv) {
+                    const double k = (double)acc_re(At, 0);
+                    if (a.mode == 1) {
+                        a.f00_out[o] = k;
+                    } else {
+                        const double* fb = reinterpret_cast<const double*>(f0row);
+                        const double tt = mul_rn(k, a.c1);
+                        const double b = fb[roff];
+                        if (a.f00_out) a.f00_out[o] = add_rn(b, tt);
+                        a.f00_A[o] = fma_rn(
+                            tt, a.c2, a.first ? b : reinterpret_cast<const double*>(f0row + L.f00_arr_bytes)[roff]);
+                    }
+                }
+                __syncwarp();
+                if (need_B && lane == 0) mbar_arrive(f0empty);
+                return;
+            }
             const int rb = rows_used & 1;
             if (need_B && !dead && !mbar_wait(rowfull + rb, (uint32_t)((rows_used >> 1) & 1), wlim)) {
                 atomicOr(a.err, 16);
                 dead = true;
             }
             if (!dead && pv) {
-                const unsigned char* base = rows + (size_t)rb * 2 * L.row_arr_bytes;
-                if (t == 0) {
-                    const double k = (double)acc_re(At, 0);
-                    if (a.mode == 1) {
-                        a.f00_out[o] = k;
-                    } else {
-                        const double tt = mul_rn(k, a.c1);
-                        const double b = reinterpret_cast<const double*>(base)[roff];
-                        if (a.f00_out) a.f00_out[o] = add_rn(b, tt);
-                        a.f00_A[o] = fma_rn(tt, a.c2,
-                                            a.first ? b : reinterpret_cast<const double*>(base + L.row_arr_bytes)[roff]);
-                    }
-                } else {
-                    const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
-                    const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
-                    store_row<MC, TS>(a, min(t, a.m0), zero, At, a.pl_out ? a.pl_out + g0 : nullptr,
-                                      a.pl_A + g0, reinterpret_cast<const TS*>(base) + roff,
-                                      reinterpret_cast<const TS*>(base + L.row_arr_bytes) + roff, rstride);
-                }
+                const unsigned char* base = rows + (size_t)rb * 2 * L.rowl_arr_bytes;
+                const bool zero = p < (t >= 2 ? min(t - 1, 80) : 0);
+                const long long g0 = (long long)splane[t * mstride] * a.pstride + o;
+                store_row<MC, TS>(a, min(t, a.m0), zero, At, a.pl_out ? a.pl_out + g0 : nullptr, a.pl_A + g0,
+                                  reinterpret_cast<const TS*>(base) + roff,
+                                  reinterpret_cast<const TS*>(base + L.rowl_arr_bytes) + roff, rstride);
             }
             __syncwarp();
             if (need_B && lane == 0) mbar_arrive(rowempty + rb);
             ++rows_used;
         };
 
-        // target row t lives in R[t % 3], I[t % 3]: source row s adds into
-        // rows s-1, s, s+1, then row s-1 is finished, stored and cleared for
-        // row s+2, with no register moves between rows
         // source row 0: f00 into row 1
         acquire();
         if (!dead) {
@@ -320,9 +353,8 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
         release();
 
         // source row s, K = s % 3
-        auto source_row = [&](auto kcst, const int s) {
-            constexpr int K = decltype(kcst)::value;
-            constexpr int KM = (K + 2) % 3, KP = (K + 1) % 3;
+        // source row s into target rows s-1 (A[0]), s (A[1]), s+1 (A[2]); then row s-1 is stored
+        auto source_row = [&](const int s) {
             const CoefT<TS>* crow = scoef + s * mstride;
             const int mtop = min(s, a.m0);
             static_for<MC + 1>([&](auto mcst) {
@@ -333,7 +365,7 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * L.slot_bytes);
                     const long long qs = splane[s * mstride + m];
                     const TS* ref = (a.pl_ref && __ldg(a.pl_keep + qs)) ? a.pl_ref + qs * np : nullptr;
-                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, ref, np);
+                    couple_src3<MC, m>(A[0], A[1], A[2], crow[m], sb, seg, nb, th, ref, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             // the current of f = ref + stored deviation
@@ -350,19 +382,19 @@ __global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<
                 }
                 release();
             });
-            epilogue(s - 1, A[KM]);
-            acc_zero(A[KM]);
+            epilogue(s - 1, A[0]);
         };
-        for (int s0 = 1; s0 <= a.l0; s0 += 3) {
-            source_row(std::integral_constant<int, 1>{}, s0);
-            if (s0 + 1 <= a.l0) source_row(std::integral_constant<int, 2>{}, s0 + 1);
-            if (s0 + 2 <= a.l0) source_row(std::integral_constant<int, 0>{}, s0 + 2);
+        // A[0], A[1], A[2] hold target rows s-1, s, s+1 while source row s is
+        // added; then row s-1 is stored and the rows move down one accumulator.
+        // One copy of the source-row code (not one per row position) keeps the
+        // consumer loop small enough for the instruction cache.
+        for (int s = 1; s <= a.l0; ++s) {
+            source_row(s);
+            A[0] = A[1];
+            A[1] = A[2];
+            acc_zero(A[2]);
         }
-        switch (a.l0 % 3) {
-            case 0: epilogue(a.l0, A[0]); break;
-            case 1: epilogue(a.l0, A[1]); break;
-            default: epilogue(a.l0, A[2]); break;
-        }
+        epilogue(a.l0, A[0]);
 
         // per-cell current: warp sums to global; stage_fields_kernel adds the
         // warps of a cell in order (deterministic) and updates E and B.  No

@@ -124,20 +124,25 @@ struct alignas(16) CoefT {
 
 // shared-memory layout (host and device agree)
 struct PipeLayout {
-    size_t off_coef, off_plane, off_fld, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
+    size_t off_coef, off_plane, off_fld, fld_stride, off_slots, slot_bytes, off_rows, row_arr_bytes, total;
+    size_t rowl_arr_bytes, off_f00, f00_arr_bytes;   // single-problem kernel's row stage
     int seg_cells;
     int depth;   // slots in the source ring (<= kMaxDepth)
 };
-// barriers at offset 0: full[kMaxDepth], empty[kMaxDepth], rowfull[2], rowempty[2]
+// barriers at offset 0: full[kMaxDepth], empty[kMaxDepth], rowfull[2], rowempty[2],
+// f00full, f00empty
+static_assert((2 * kMaxDepth + 6) * sizeof(uint64_t) <= 256, "barrier area");
 __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, bool has_y, int elem_bytes, int m0,
                                                  int depth = kDepth) {
     PipeLayout L;
     L.seg_cells = tx + 2 + (has_y ? 2 * tx : 0);
     L.off_coef = 256;
     L.off_plane = align_up(L.off_coef + (size_t)16 * elem_bytes * ncoef, 16);
-    // fields of the tile's cells, [2 tiles][6][tx] (single-problem kernel)
+    // fields of the tile's cells (single-problem kernel), [2 tiles][6 fields]:
+    // each the 16-byte aligned span of memory holding the tile's values
     L.off_fld = align_up(L.off_plane + sizeof(int) * (size_t)ncoef, 16);
-    L.off_slots = align_up(L.off_fld + sizeof(double) * 2 * 6 * (size_t)tx, 128);
+    L.fld_stride = align_up((size_t)tx * elem_bytes + 32, 16);
+    L.off_slots = align_up(L.off_fld + 2 * 6 * L.fld_stride, 128);
     // a slot holds one harmonic: Re and Im planes of the TS type, or the FP64 f00 plane
     const size_t plane_part = (size_t)2 * L.seg_cells * np * elem_bytes;
     const size_t f00_part = (size_t)L.seg_cells * np * 8;
@@ -146,8 +151,16 @@ __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, boo
     L.off_rows = L.off_slots + (size_t)depth * L.slot_bytes;
     const size_t row0 = (size_t)tx * np * 8;
     const size_t rowl = (size_t)(1 + 2 * m0) * tx * np * elem_bytes;
+    // batched kernel: every target row, f00 included, passes the double-buffered row stage
     L.row_arr_bytes = align_up(row0 > rowl ? row0 : rowl, 128);
-    L.total = L.off_rows + 2 * 2 * L.row_arr_bytes;   // [buffer][B, A]
+    // single-problem kernel: rows l >= 1 pass the double-buffered stage
+    // [buffer][B, A]; the f00 row (and the tile's fields) have their own
+    // buffer [B, A], refilled for the next tile once row 0 is stored, so
+    // they arrive a whole tile ahead instead of at the tile boundary
+    L.rowl_arr_bytes = align_up(rowl, 128);
+    L.f00_arr_bytes = align_up(row0, 128);
+    L.off_f00 = L.off_rows + 2 * 2 * L.rowl_arr_bytes;
+    L.total = L.off_f00 + 2 * L.f00_arr_bytes;
     return L;
 }
 
@@ -820,7 +833,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
             ++rows_used;
         };
 
-        // target row t lives in R[t % 3], I[t % 3] (no register moves between rows)
+        // target row t is in A[0] (row s-1), A[1] (row s) or A[2] (row s+1) while source row s is added
         // source row 0: f00 (already acquired) into row 1
         if (!dead) {
             const double* sb = reinterpret_cast<const double*>(slots + (size_t)slot * P.slot_stride + P.hdr);
@@ -828,10 +841,8 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
         }
         release();
 
-        // source row s, K = s % 3
-        auto source_row = [&](auto kcst, const int s) {
-            constexpr int K = decltype(kcst)::value;
-            constexpr int KM = (K + 2) % 3, KP = (K + 1) % 3;
+        // source row s into target rows s-1 (A[0]), s (A[1]), s+1 (A[2]); then row s-1 is stored
+        auto source_row = [&](const int s) {
             const CoefT<TS>* crow = scoef + s * mstride;
             const int mtop = min(s, a.m0);
             static_for<MC + 1>([&](auto mcst) {
@@ -842,7 +853,7 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
                     const TS* sb = reinterpret_cast<const TS*>(slots + (size_t)slot * P.slot_stride + P.hdr);
                     const long long qs = splane[s * mstride + m];
                     const TS* ref = (a.pl_ref && __ldg(a.pl_keep + qs)) ? a.pl_ref + qs * np : nullptr;
-                    couple_src3<MC, m>(A[KM], A[K], A[KP], crow[m], sb, seg, nb, th, ref, np);
+                    couple_src3<MC, m>(A[0], A[1], A[2], crow[m], sb, seg, nb, th, ref, np);
                     if constexpr (m <= 1) {
                         if (s == 1) {
                             // the current of f = ref + stored deviation
@@ -859,19 +870,17 @@ __global__ void __launch_bounds__(MAXT, batch_min_blocks<MC, MAXT>())
                 }
                 release();
             });
-            epilogue(s - 1, A[KM]);
-            acc_zero(A[KM]);
+            epilogue(s - 1, A[0]);
         };
-        for (int s0 = 1; s0 <= a.l0; s0 += 3) {
-            source_row(std::integral_constant<int, 1>{}, s0);
-            if (s0 + 1 <= a.l0) source_row(std::integral_constant<int, 2>{}, s0 + 1);
-            if (s0 + 2 <= a.l0) source_row(std::integral_constant<int, 0>{}, s0 + 2);
+        // the rows move down one accumulator after each source row (one copy
+        // of the source-row code keeps the loop within the instruction cache)
+        for (int s = 1; s <= a.l0; ++s) {
+            source_row(s);
+            A[0] = A[1];
+            A[1] = A[2];
+            acc_zero(A[2]);
         }
-        switch (a.l0 % 3) {
-            case 0: epilogue(a.l0, A[0]); break;
-            case 1: epilogue(a.l0, A[1]); break;
-            default: epilogue(a.l0, A[2]); break;
-        }
+        epilogue(a.l0, A[0]);
 
         // per-cell current: warp sums to the problem's partial-sum array;
         // the batched field kernel adds the warps of a cell in order
