@@ -847,30 +847,43 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
         j = 0;
         do { ++l; } while (l <= l0 && !collided(a, l, 0));
     };
-    auto load_batch = [&](long long cell, int l, int j, double (&r)[P][E]) {
+    // a batch's rows as stored: the next batch's loads stay in flight during
+    // this batch's solve in the storage type (FP32 planes take half the
+    // registers of their FP64 values) ...
+    auto load_raw = [&](long long cell, int l, int j, TP (&r)[P][E]) {
         if (l > l0) return;
         const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
         const long long q0 = a.plane_of[l * (a.m0 + 1)] + j;
 #pragma unroll
         for (int b = 0; b < P; ++b) {
             const TP* g = planes + (q0 + b) * a.pstride + cell * n;
+#pragma unroll
+            for (int e = 0; e < E; ++e) r[b][e] = (j + b < nq && i0 + e < n) ? g[i0 + e] : TP(0);
+        }
+    };
+    // ... and widened to FP64, the plane's profile added, when the batch is solved
+    auto widen = [&](int l, int j, const TP (&r)[P][E], double (&d)[P][E]) {
+        const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
+        const long long q0 = a.plane_of[l * (a.m0 + 1)] + j;
+#pragma unroll
+        for (int b = 0; b < P; ++b) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) d[b][e] = (double)r[b][e];
             const float* rp = (j + b < nq) ? ref_row<TP>(a, q0 + b) : nullptr;
             if (rp) {
 #pragma unroll
                 for (int e = 0; e < E; ++e)
-                    r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] + (double)__ldg(rp + i0 + e) : 0.0;
-            } else {
-#pragma unroll
-                for (int e = 0; e < E; ++e) r[b][e] = (j + b < nq && i0 + e < n) ? (double)g[i0 + e] : 0.0;
+                    if (i0 + e < n) d[b][e] += (double)__ldg(rp + i0 + e);
             }
         }
     };
 
-    double cur[P][E], nxt[P][E];
+    TP raw[P][E];
+    double cur[P][E];
     {
         int bl, bj;
         batch_first(bl, bj);
-        if (solve) load_batch(cell, bl, bj, cur);   // in flight during the e-e step
+        if (solve) load_raw(cell, bl, bj, raw);   // in flight during the e-e step
         for (int k = lane; k < n; k += 32) s.f[k] = a.f00[cell * n + k];
         __syncwarp();
         if (a.do_ee) {
@@ -905,12 +918,13 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
 
         int cl = -1;   // l of the per-l constants below
         double id[E], cp[E], Af[5], Ab[5];
+        if (bl <= l0) widen(bl, bj, raw, cur);
         while (bl <= l0) {
             const int l = bl, j = bl <= l0 ? bj : 0;
             const int nq = 1 + 2 * min(min(l, a.m0), a.mmax_coll);
             int nl = bl, nj = bj;
             batch_next(nl, nj);
-            if (nl <= l0) load_batch(cell, nl, nj, nxt);
+            if (nl <= l0) load_raw(cell, nl, nj, raw);
             if (l != cl) {
                 // per-l constants: pivots of this lane's run and the scan multipliers
                 cl = l;
@@ -1006,10 +1020,7 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
                     }
                 }
             }
-#pragma unroll
-            for (int b = 0; b < P; ++b)
-#pragma unroll
-                for (int e = 0; e < E; ++e) cur[b][e] = nxt[b][e];
+            if (nl <= l0) widen(nl, nj, raw, cur);
             bl = nl; bj = nj;
         }
         __syncwarp();
