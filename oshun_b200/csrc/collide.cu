@@ -625,6 +625,43 @@ __device__ void ee_substeps(const CollideArgs& a, const Smem& s) {
     }
 }
 
+// The same substeps with the four slopes from one call site of ee_slope:
+// one inlined copy of its scans and logarithms instead of four, for the lane
+// kernels of short rows (the stage updates are the ones above)
+__device__ void ee_substeps_one_site(const CollideArgs& a, const Smem& s) {
+    const StepP sp = step_params(a);
+    const int n = a.np;
+    const int lane = threadIdx.x & 31;
+    for (int sub = 0; sub < sp.nsub; ++sub) {
+        const double h = sp.hsub;
+        for (int k = lane; k < n; k += 32) { s.f0[k] = s.f[k]; s.f1[k] = s.f[k]; }
+        __syncwarp();
+        for (int st = 0; st < 4; ++st) {
+            ee_slope(a, s, st == 3 ? s.f0 : s.f1, s.fh);
+            if (st == 0) {
+                for (int k = lane; k < n; k += 32) {
+                    double t = s.fh[k] * (0.5 * h);
+                    s.f1[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
+                }
+            } else if (st == 1) {
+                for (int k = lane; k < n; k += 32) {
+                    s.f1[k] = s.f0[k];
+                    double t = s.fh[k] * (0.5 * h);
+                    s.f1[k] += t; t *= 2.0 / 3.0; s.f[k] += t;
+                }
+            } else if (st == 2) {
+                for (int k = lane; k < n; k += 32) {
+                    double t = s.fh[k] * h;
+                    s.f0[k] += t; t *= 1.0 / 3.0; s.f[k] += t;
+                }
+            } else {
+                for (int k = lane; k < n; k += 32) s.f[k] += s.fh[k] * (h / 6.0);
+            }
+            __syncwarp();
+        }
+    }
+}
+
 // the backward-Euler e-e step alone, one warp per cell (the collision
 // kernels then run with do_ee = 0)
 __global__ void __launch_bounds__(32) ee_implicit_kernel(const CollideArgs a) {
@@ -887,7 +924,8 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
         for (int k = lane; k < n; k += 32) s.f[k] = a.f00[cell * n + k];
         __syncwarp();
         if (a.do_ee) {
-            ee_substeps(a, s);
+            if constexpr (E <= 3) ee_substeps_one_site(a, s);
+            else ee_substeps(a, s);
             for (int k = lane; k < n; k += 32) a.f00[cell * n + k] = s.f[k];
         }
         if (!solve) return;
@@ -1027,8 +1065,12 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
     }
 }
 
+// rows of up to 96 points (E <= 3) leave 12.3 KB of shared memory per cell:
+// the kernel is held to 128 registers so that 16 cells are resident per SM
+template <int E>
+constexpr int lane_min_blocks() { return E <= 3 ? 16 : 1; }
 template <typename TP, int E, int P>
-__global__ void __launch_bounds__(32) collide_lane_kernel(const CollideArgs a) {
+__global__ void __launch_bounds__(32, lane_min_blocks<E>()) collide_lane_kernel(const CollideArgs a) {
     extern __shared__ double smem[];
     for (long long cell = blockIdx.x; cell < a.cells; cell += gridDim.x) collide_lane_cell<TP, E, P>(a, cell, smem);
 }
