@@ -8,8 +8,15 @@
 namespace oshun {
 namespace {
 
+// CTAs per SM the kernel is compiled for: two for m0 = 0 (few accumulators,
+// 80 registers a thread, half-size ring slots) and at most 384 threads, so
+// that one CTA's tile starts and ends overlap the other's work
+template <int MC, int MAXT>
+constexpr int tile_min_blocks() { return (MC == 0 && MAXT <= 384) ? 2 : 1; }
+
 template <int MC, typename TS, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1) rk_stage_tile_kernel(const StageArgs<TS> a, const int D) {
+__global__ void __launch_bounds__(MAXT, tile_min_blocks<MC, MAXT>())
+    rk_stage_tile_kernel(const StageArgs<TS> a, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int np = a.np, nx = a.nx, ny = a.ny;
     const int np_pad = (np + 31) & ~31;
@@ -433,8 +440,17 @@ cudaError_t launch_tile(const StageArgs<TS>& a, int tx, const PipeLayout& L, cud
     }
     const int np_pad = ((a.np + 31) / 32) * 32;
     const long long tiles = (long long)a.ny * ((a.nx + tx - 1) / tx);
-    // one resident CTA per SM, each walking tiles blockIdx.x + k gridDim.x
-    const long long blocks = tiles < sm_count() ? tiles : sm_count();
+    // as many CTAs as are resident at once (one per SM, two for the m0 = 0
+    // form when its shared memory allows), each walking tiles blockIdx.x + k gridDim.x
+    int per_sm = 1;
+    if (tile_min_blocks<MC, MAXT>() > 1) {
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, rk_stage_tile_kernel<MC, TS, MAXT>, np_pad * tx + 64, L.total);
+        if (e != cudaSuccess || per_sm < 1) { (void)cudaGetLastError(); per_sm = 1; }
+        if (per_sm > tile_min_blocks<MC, MAXT>()) per_sm = tile_min_blocks<MC, MAXT>();
+    }
+    const long long resident = (long long)sm_count() * per_sm;
+    const long long blocks = tiles < resident ? tiles : resident;
     rk_stage_tile_kernel<MC, TS, MAXT><<<dim3((unsigned)blocks), dim3(np_pad * tx + 64), L.total, s>>>(a, L.depth);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -455,7 +471,8 @@ cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
     //   FP64 with m0 <= 6, FP32 with m0 >= 7    up to 320 (12 warps)
     //   FP64 with m0 >= 7 (spills at 168)       up to 192 (8 warps, 255)
     constexpr bool f32 = sizeof(TS) == 4;
-    constexpr int budget = (MC <= 1 || (f32 && MC <= 6)) ? 448 : (f32 || MC <= 6) ? 320 : 192;
+    // m0 = 0: up to 320 consumer threads, two CTAs per SM (tile_min_blocks)
+    constexpr int budget = MC == 0 ? 320 : (MC <= 1 || (f32 && MC <= 6)) ? 448 : (f32 || MC <= 6) ? 320 : 192;
     int tx = budget >= np_pad ? budget / np_pad : 1;
     if (tx > kMaxTx) tx = kMaxTx;
     if (tx > a.nx) tx = a.nx;
@@ -464,17 +481,25 @@ cudaError_t pipe_mc(const StageArgs<TS>& a, cudaStream_t s) {
     const long long per_sm = cells / sm_count();
     if (tx > per_sm) tx = per_sm > 1 ? (int)per_sm : 1;
     const int ncoef = (a.l0 + 1) * (a.m0 + 1);
-    // the deepest source ring that fits (4 slots at least), else fewer cells a tile
+    // the deepest source ring that fits `cap` (4 slots at least), else fewer cells a tile
+    auto plan = [&](size_t cap, PipeLayout& L, int& t) -> bool {
+        t = tx;
+        for (;;) {
+            int depth = kDepth;
+            L = pipe_layout(ncoef, t, a.np, a.ny > 1, (int)sizeof(TS), a.m0, depth);
+            while (L.total > cap && depth > 4)
+                L = pipe_layout(ncoef, t, a.np, a.ny > 1, (int)sizeof(TS), a.m0, --depth);
+            if (L.total <= cap || t == 1) break;
+            --t;
+        }
+        return L.total <= cap;
+    };
+    // m0 = 0: half an SM's shared memory, so that two CTAs share it, when
+    // that still leaves 4 slots; otherwise the whole of it
     PipeLayout L;
-    for (;;) {
-        int depth = kDepth;
-        L = pipe_layout(ncoef, tx, a.np, a.ny > 1, (int)sizeof(TS), a.m0, depth);
-        while (L.total > kSmemMax && depth > 4)
-            L = pipe_layout(ncoef, tx, a.np, a.ny > 1, (int)sizeof(TS), a.m0, --depth);
-        if (L.total <= kSmemMax || tx == 1) break;
-        --tx;
-    }
-    if (L.total > kSmemMax) return cudaErrorNotSupported;
+    int txp = tx;
+    if (!(MC == 0 && plan(kSmemHalf, L, txp)) && !plan(kSmemMax, L, txp)) return cudaErrorNotSupported;
+    tx = txp;
     const int threads = np_pad * tx + 64;
     if (threads <= 256) return launch_tile<MC, TS, 256>(a, tx, L, s);
     if (threads <= 384) return launch_tile<MC, TS, 384>(a, tx, L, s);

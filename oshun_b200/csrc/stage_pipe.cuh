@@ -59,6 +59,7 @@ constexpr int kMaxDepth = 12;                 // ring slots the barrier area hol
 constexpr unsigned long long kWaitNs = 1000000000ull;   // a pipeline wait gives up after 1 s
 constexpr int kMaxTx = 8;
 constexpr size_t kSmemMax = 227 * 1024;          // dynamic shared memory of one CTA
+constexpr size_t kSmemHalf = (228 * 1024 - 2 * 1024) / 2;   // each of two CTAs on one SM (1 KB reserved each)
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
@@ -143,8 +144,9 @@ __host__ __device__ inline PipeLayout pipe_layout(int ncoef, int tx, int np, boo
     L.off_fld = align_up(L.off_plane + sizeof(int) * (size_t)ncoef, 16);
     L.fld_stride = align_up((size_t)tx * elem_bytes + 32, 16);
     L.off_slots = align_up(L.off_fld + 2 * 6 * L.fld_stride, 128);
-    // a slot holds one harmonic: Re and Im planes of the TS type, or the FP64 f00 plane
-    const size_t plane_part = (size_t)2 * L.seg_cells * np * elem_bytes;
+    // a slot holds one harmonic: Re and Im planes of the TS type (Re alone
+    // when m0 = 0: every source is real), or the FP64 f00 plane
+    const size_t plane_part = (size_t)(m0 > 0 ? 2 : 1) * L.seg_cells * np * elem_bytes;
     const size_t f00_part = (size_t)L.seg_cells * np * 8;
     L.slot_bytes = align_up(plane_part > f00_part ? plane_part : f00_part, 128);
     L.depth = depth;
