@@ -831,10 +831,11 @@ __global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
 
 // Tridiagonal collision step for nump <= 32 E, one warp per cell (1-warp
 // CTAs, grid-stride over cells), rows in registers:
-//   1. f00 e-e substeps and reset_coeff as above; then the Thomas pivots of
-//      every l, one lane per l: c'_i and 1/(b_i - c'_{i-1} a_i)
-//      (TridiagonalSolve, def-Nmethods.cpp:152-159), 1/b_0 at i = 0.
-//   2. the collided planes of one l in batches of P: lane j holds p in
+//   1. f00 e-e substeps and reset_coeff as above.
+//   2. per collided l, the Thomas pivots of each lane's run of p (c'_i and
+//      1/(b_i - c'_{i-1} a_i), 1/b_0 at i = 0; TridiagonalSolve,
+//      def-Nmethods.cpp:152-159) from a warp scan of the pivot recurrence
+//      (lane_pivots); then the collided planes of that l in batches of P: lane j holds p in
 //      [jE, jE+E) of each row in registers (the next batch's rows are loaded
 //      while this one is solved).  Both recurrences of TridiagonalSolve --
 //      d'_i = (d_i - a_i d'_{i-1}) / (b_i - c'_{i-1} a_i) forward,
@@ -844,8 +845,7 @@ __global__ void __launch_bounds__(32) collide_warp_kernel(const CollideArgs a) {
 //      multipliers depend on l only, so their composition and scan are done
 //      once per l and only the offsets are scanned per plane.
 // Shared memory (doubles): 4 scalars, tri_a, tri_b, tri_c, scat, then the
-// e-e/reset work arrays, which the per-l pivots overwrite once reset_coeff
-// is done.
+// e-e/reset work arrays (the pivots stay in registers, per l).
 __device__ Smem carve_lane(double* base, int np) {
     Smem s;
     s.sc = base;
@@ -853,12 +853,80 @@ __device__ Smem carve_lane(double* base, int np) {
     s.df0 = s.scat + np; s.ddf0 = s.df0 + np;
     s.f = s.ddf0 + np; s.f0 = s.f + np; s.f1 = s.f0 + np; s.fh = s.f1 + np;
     s.I4 = s.fh + np; s.I2 = s.I4 + np; s.J1 = s.I2 + np;
-    s.chunk = s.df0;   // pivots: [l-1][c' (np), 1/pivot (np)]
+    s.chunk = nullptr;
     return s;
 }
-__host__ __device__ inline size_t lane_smem_doubles(int np, int l0) {
-    const size_t work = 9 * (size_t)np, piv = 2 * (size_t)l0 * np;
-    return 4 + 4 * (size_t)np + (work > piv ? work : piv);
+__host__ __device__ inline size_t lane_smem_doubles(int np, int /*l0*/) {
+    return 4 + 13 * (size_t)np;   // scalars, tri_a/b/c, scat, e-e and reset work arrays
+}
+
+// Thomas pivots of harmonic order l for this lane's run of p, c'_i and
+// 1/(b_i - c'_{i-1} a_i), with b_i = tri_b_i + 1 - ll1 scat_i (tri_b_0 left
+// out for l > 1), as TridiagonalSolve forms them (def-Nmethods.cpp:152-159).
+// c'_i = c_i / (b_i - a_i c'_{i-1}) is a linear-fractional map of c'_{i-1},
+// the 2x2 matrix [[0, c_i], [-a_i, b_i]] acting on (c'_{i-1}, 1): each lane
+// composes its run's matrices, a warp scan of the products (rescaled by
+// powers of two, which leaves the maps unchanged) gives the value entering
+// the run, and the lane applies the recursion inside its run.  No per-l
+// table is kept, so a cell needs 4 + 13 np doubles of shared memory.
+struct M22 {
+    double a, b, c, d;
+};
+__device__ __forceinline__ M22 m22_mul(const M22& x, const M22& y) {
+    return M22{fma(x.a, y.a, x.b * y.c), fma(x.a, y.b, x.b * y.d), fma(x.c, y.a, x.d * y.c),
+               fma(x.c, y.b, x.d * y.d)};
+}
+__device__ __forceinline__ M22 m22_rescale(M22 x) {
+    const double mx = fmax(fmax(fabs(x.a), fabs(x.b)), fmax(fabs(x.c), fabs(x.d)));
+    const int ex = (int)((__double_as_longlong(mx) >> 52) & 0x7ff);
+    if (mx > 0.0 && ex > 0 && ex < 0x7ff) {
+        const double sc = __longlong_as_double((long long)(2046 - ex) << 52);   // 2^(1023 - ex)
+        x.a *= sc; x.b *= sc; x.c *= sc; x.d *= sc;
+    }
+    return x;
+}
+template <int E>
+__device__ __forceinline__ void lane_pivots(const Smem& s, const int l, const int n, const int i0, double (&cp)[E],
+                                            double (&id)[E]) {
+    const int lane = threadIdx.x & 31;
+    const double ll1 = l * ((-0.5) * (l + 1.0));
+    double b[E];
+    M22 m{1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int i = i0 + e;
+        b[e] = 1.0;
+        if (i < n) {
+            b[e] = (i == 0 && l > 1 ? 0.0 : s.tri_b[i]) + (1.0 - ll1 * s.scat[i]);
+            m = m22_mul(M22{0.0, s.tri_c[i], -s.tri_a[i], b[e]}, m);
+        }
+    }
+    m = m22_rescale(m);
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const M22 o{__shfl_up_sync(kFull, m.a, off), __shfl_up_sync(kFull, m.b, off),
+                    __shfl_up_sync(kFull, m.c, off), __shfl_up_sync(kFull, m.d, off)};
+        if (lane >= off) m = m22_rescale(m22_mul(m, o));
+    }
+    const double xb = __shfl_up_sync(kFull, m.b, 1), xd = __shfl_up_sync(kFull, m.d, 1);
+    double cprev = lane == 0 ? 0.0 : xb / xd;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int i = i0 + e;
+        if (i < n) {
+            if (i == 0) {
+                id[e] = 1.0 / b[e];
+                cprev = s.tri_c[0] / b[e];
+            } else {
+                id[e] = 1.0 / (b[e] - cprev * s.tri_a[i]);
+                cprev = s.tri_c[i] * id[e];
+            }
+            cp[e] = cprev;
+        } else {
+            id[e] = 0.0;
+            cp[e] = 0.0;
+        }
+    }
 }
 
 template <typename TP, int E, int P>
@@ -869,7 +937,6 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
     TP* planes = reinterpret_cast<TP*>(a.planes);
     const bool solve = a.do_l1 || a.do_lm;
     const Smem s = carve_lane(smem, n);
-    double* piv = s.chunk;
     const int i0 = lane * E;   // first p of this lane's run
 
     // plane batches: l, first plane, count (planes of one l are consecutive)
@@ -930,25 +997,6 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
         }
         if (!solve) return;
         flm_reset(a, s, s.f);
-        // pivots of every collided l, one lane per l
-        for (int l = 1 + lane; l <= l0; l += 32) {
-            if (!collided(a, l, 0)) continue;
-            const double ll1 = l * ((-0.5) * (l + 1.0));
-            double* cpl = piv + (size_t)(l - 1) * 2 * n;
-            double* idl = cpl + n;
-            const double b0 = (l > 1 ? 0.0 : s.tri_b[0]) + (1.0 - ll1 * s.scat[0]);
-            double cprev = s.tri_c[0] / b0;
-            cpl[0] = cprev;
-            idl[0] = 1.0 / b0;
-            for (int i = 1; i < n; ++i) {
-                const double bi = s.tri_b[i] + (1.0 - ll1 * s.scat[i]);
-                const double id = 1.0 / (bi - cprev * s.tri_a[i]);
-                cprev = s.tri_c[i] * id;
-                cpl[i] = cprev;
-                idl[i] = id;
-            }
-        }
-        __syncwarp();
         // this lane's tri_a (forward multiplier -a_i id_i)
         double ta[E];
 #pragma unroll
@@ -966,14 +1014,11 @@ __device__ __forceinline__ void collide_lane_cell(const CollideArgs& a, const lo
             if (l != cl) {
                 // per-l constants: pivots of this lane's run and the scan multipliers
                 cl = l;
-                const double* cpl = piv + (size_t)(l - 1) * 2 * n;
-                const double* idl = cpl + n;
+                lane_pivots<E>(s, l, n, i0, cp, id);
                 double A = 1.0, B = 1.0;
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     const int i = i0 + e;
-                    id[e] = i < n ? idl[i] : 0.0;
-                    cp[e] = i < n ? cpl[i] : 0.0;
                     if (i < n) A = (i == 0) ? 0.0 : A * (-(ta[e] * id[e]));
                 }
 #pragma unroll
