@@ -330,6 +330,11 @@ int oshun_batch_autotune(oshun_batch b, int steps, int* stage_threads, int* tile
 typedef struct oshun_adj_ctx* oshun_adjoint;
 int oshun_adjoint_create(const oshun_cfg* cfg, oshun_adjoint* out);
 int oshun_adjoint_destroy(oshun_adjoint a);
+/* Without a stream set, oshun_adjoint_forward and oshun_adjoint_vjp run on
+ * the handle's own stream and return when their results are written.  With a
+ * caller's stream set (non-null), both are queued on that stream and return
+ * without waiting: the caller orders its own reads and writes of the vectors
+ * on the same stream.  A null stream restores the waiting form. */
 int oshun_adjoint_set_stream(oshun_adjoint a, void* stream);
 int oshun_adjoint_state_size(oshun_adjoint a, long long* n);
 /* y_next = step(y) through the production kernels */

@@ -24,8 +24,11 @@ from .abi import OshunError, load, make_cfg
 
 
 class Run:
-    """One oshun_adjoint handle (its own stream; every call waits for torch's
-    current stream first and returns synchronized)."""
+    """One oshun_adjoint handle.  Called on a torch stream other than the
+    default one, the handle's calls are queued on that same stream and do not
+    wait (the torch operations around them are ordered by the stream); on the
+    default stream every call waits for torch's work first and returns
+    synchronized."""
 
     def __init__(self, **cfg):
         self.lib = load()
@@ -37,6 +40,7 @@ class Run:
         self._check(self.lib.oshun_adjoint_state_size(self._a, ctypes.byref(n)), "oshun_adjoint_state_size")
         self.n = n.value
         self.dt = self.cfg.dt
+        self._stream = 0   # the torch stream the handle's calls are queued on (0: none, they wait)
 
     def _check(self, rc, what):
         if rc != 0:
@@ -53,17 +57,29 @@ class Run:
         except Exception:
             pass
 
+    def _order(self):
+        """Queue the handle's calls on torch's current stream when it is not
+        the default stream; otherwise wait for torch's work (the calls wait too)."""
+        cur = torch.cuda.current_stream()
+        if cur.cuda_stream != self._stream:
+            self._check(self.lib.oshun_adjoint_set_stream(self._a, ctypes.c_void_p(cur.cuda_stream or None)),
+                        "oshun_adjoint_set_stream")
+            self._stream = cur.cuda_stream
+        if self._stream == 0:
+            cur.synchronize()
+
     def forward(self, y: torch.Tensor, clocks, collisions: bool = True) -> torch.Tensor:
         out = torch.empty_like(y)
-        torch.cuda.current_stream().synchronize()   # y written by torch; the handle's calls end synchronized
+        self._order()
         self._check(self.lib.oshun_adjoint_forward(self._a, y.data_ptr(), out.data_ptr(), int(collisions), *clocks),
                     "oshun_adjoint_forward")
         return out
 
     def vjp(self, y: torch.Tensor, lam_next: torch.Tensor, clocks, collisions: bool = True) -> torch.Tensor:
         lam = torch.empty_like(y)
-        torch.cuda.current_stream().synchronize()
-        self._check(self.lib.oshun_adjoint_vjp(self._a, y.data_ptr(), lam_next.contiguous().data_ptr(),
+        lam_next = lam_next.contiguous()
+        self._order()
+        self._check(self.lib.oshun_adjoint_vjp(self._a, y.data_ptr(), lam_next.data_ptr(),
                                                lam.data_ptr(), int(collisions), *clocks), "oshun_adjoint_vjp")
         return lam
 

@@ -236,6 +236,9 @@ __global__ void profile_final_kernel(const double2* __restrict__ part, const int
 }
 
 __global__ void clock_advance_kernel(Clock* c, double dt) { c->t += dt; }
+__global__ void clock_set_kernel(Clock* c, double t, double t_ee, double t_eb) {
+    c->t = t; c->t_ee = t_ee; c->t_eb = t_eb;
+}
 __global__ void clock_commit_kernel(Clock* c, int ee, int eb) {
     if (ee) c->t_ee = c->t;
     if (eb) c->t_eb = c->t;
@@ -981,6 +984,48 @@ void free_ctx(oshun_ctx* h) {
 
 }  // namespace
 
+namespace {
+// nsteps small steps on the device clock, queued on the handle's stream
+// without waiting (one captured graph per state parity)
+int enqueue_steps(oshun_ctx* h, int nsteps, int collisions) {
+    for (int s = 0; s < nsteps; ++s) {
+        // one graph per state parity: RK4 stages, clocks, collision step
+        cudaGraphExec_t& g = h->graph[h->cur][collisions];
+        if (!g && h->graphs_ok) {
+            const int cur0 = h->cur;
+            cudaGraph_t graph = nullptr;
+            bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            int rc = ok ? enqueue_step_device(h, collisions) : OSHUN_OK;
+            h->cur = cur0;
+            if (ok) ok = cudaStreamEndCapture(h->stream, &graph) == cudaSuccess && rc == OSHUN_OK;
+            if (ok) ok = cudaGraphInstantiate(&g, graph, 0) == cudaSuccess;
+            if (graph) cudaGraphDestroy(graph);
+            if (!ok) {
+                // capture unavailable on this stream: plain launches from now on
+                (void)cudaGetLastError();
+                if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+                h->graphs_ok = false;
+                if (rc) return rc;
+            }
+        }
+        if (g) {
+            CK(cudaGraphLaunch(g, h->stream));
+            h->cur ^= 1;
+        } else {
+            int rc = enqueue_step_device(h, collisions);
+            if (rc) return rc;
+        }
+        h->t += h->cfg.dt;
+        if (collisions) {
+            h->t_ee = h->t;
+            h->t_eb = h->t;
+        }
+    }
+    return OSHUN_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int oshun_abi_version(void) { return OSHUN_ABI_VERSION; }
@@ -1248,39 +1293,7 @@ int oshun_step(oshun_handle h, int nsteps, int collisions) {
     collisions = collisions ? 1 : 0;
     Clock ck{h->t, h->t_ee, h->t_eb};
     CK(cudaMemcpyAsync(h->d_clock, &ck, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
-    for (int s = 0; s < nsteps; ++s) {
-        // one graph per state parity: RK4 stages, clocks, collision step
-        cudaGraphExec_t& g = h->graph[h->cur][collisions];
-        if (!g && h->graphs_ok) {
-            const int cur0 = h->cur;
-            cudaGraph_t graph = nullptr;
-            bool ok = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
-            int rc = ok ? enqueue_step_device(h, collisions) : OSHUN_OK;
-            h->cur = cur0;
-            if (ok) ok = cudaStreamEndCapture(h->stream, &graph) == cudaSuccess && rc == OSHUN_OK;
-            if (ok) ok = cudaGraphInstantiate(&g, graph, 0) == cudaSuccess;
-            if (graph) cudaGraphDestroy(graph);
-            if (!ok) {
-                // capture unavailable on this stream: plain launches from now on
-                (void)cudaGetLastError();
-                if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-                h->graphs_ok = false;
-                if (rc) return rc;
-            }
-        }
-        if (g) {
-            CK(cudaGraphLaunch(g, h->stream));
-            h->cur ^= 1;
-        } else {
-            int rc = enqueue_step_device(h, collisions);
-            if (rc) return rc;
-        }
-        h->t += h->cfg.dt;
-        if (collisions) {
-            h->t_ee = h->t;
-            h->t_eb = h->t;
-        }
-    }
+    if (int rc = enqueue_steps(h, nsteps, collisions)) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return OSHUN_OK;
 }
@@ -2244,6 +2257,7 @@ struct oshun_adj_ctx {
     bool general = false;            // a 2D grid or m0 > 0: the general stage transpose
     double* ws = nullptr;
     long long ws_cap = 0;            // doubles
+    bool async = false;              // a caller's stream is set: calls are queued on it and do not wait
 };
 
 namespace {
@@ -2386,7 +2400,9 @@ int oshun_adjoint_destroy(oshun_adjoint a) {
 
 int oshun_adjoint_set_stream(oshun_adjoint a, void* stream) {
     if (!a) return OSHUN_ERR_ARG;
-    return oshun_set_stream(a->h, stream);
+    const int rc = oshun_set_stream(a->h, stream);
+    a->async = rc == OSHUN_OK && stream != nullptr;
+    return rc;
 }
 
 int oshun_adjoint_state_size(oshun_adjoint a, long long* n) {
@@ -2402,6 +2418,13 @@ int oshun_adjoint_forward(oshun_adjoint a, const double* y, double* y_next, int 
     int rc = adj_copy_in(h, h->cur, y);
     if (rc) return rc;
     h->t = t; h->t_ee = t_ee; h->t_eb = t_eb;
+    if (a->async) {
+        // queued on the caller's stream: the clock set by a kernel, no wait
+        clock_set_kernel<<<1, 1, 0, h->stream>>>(h->d_clock, t, t_ee, t_eb);
+        CK(cudaGetLastError());
+        if ((rc = enqueue_steps(h, 1, collisions ? 1 : 0))) return rc;
+        return adj_copy_out(h, h->cur, y_next);
+    }
     if ((rc = oshun_step(h, 1, collisions))) return rc;
     if ((rc = adj_copy_out(h, h->cur, y_next))) return rc;
     CK(cudaStreamSynchronize(h->stream));
@@ -2460,7 +2483,7 @@ int oshun_adjoint_vjp(oshun_adjoint a, const double* y, const double* lam_next, 
         CK(launch_rk_combine(a->acc, a->acc, 1.0, a->a, 1.0, nullptr, 0.0, n, h->stream));
     }
     CK(cudaMemcpyAsync(lam, a->acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
+    if (!a->async) CK(cudaStreamSynchronize(h->stream));
     return OSHUN_OK;
 }
 

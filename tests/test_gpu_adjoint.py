@@ -134,6 +134,31 @@ def test_checkpointed_gradient_small(oracle):
     assert np.max(np.abs(g[comps] - fd_ref)) <= 1e-5 * scale, (g[comps], fd_ref)
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_gradient_on_a_torch_stream_matches_waiting_form(prec):
+    """On a non-default torch stream the handle's calls are queued on that
+    stream without waiting: the loss and gradient are bitwise those of the
+    waiting form (same kernels, same order), and a second run on the same
+    stream reproduces them."""
+    import torch
+    cfg, tau = _small_cfg()
+    cfg = dict(cfg, precision=prec)
+    tt = torch.tensor(tau, device="cuda")
+    run0 = _run(cfg)
+    q0, g0 = _loss(run0, cfg, tt, 30, 7, 16, grad=True)     # default stream: every call waits
+    run0.close()
+    run1 = _run(cfg)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        q1, g1 = _loss(run1, cfg, tt, 30, 7, 16, grad=True)
+        q2, g2 = _loss(run1, cfg, tt, 30, 7, 16, grad=True)
+    torch.cuda.synchronize()
+    run1.close()
+    assert q1 == q0 and q2 == q0, (q0, q1, q2)
+    assert np.array_equal(g1, g0) and np.array_equal(g2, g0)
+
+
 def test_sensitivity_full_size():
     import torch
     from oshun_b200 import workloads
